@@ -1,0 +1,183 @@
+// Step orchestration: hexcore/driver.py:3314 DryDycoreDriver.step with the
+// v8.4.1 subcycle of hexcore/driver.py:2710, as a fixed sequence of kernel
+// launches on one stream (capturable into one CUDA graph).
+
+struct Launcher {
+  HexCtx& ctx;
+  cudaStream_t st;
+  long long count = 0;
+  cudaError_t err = cudaSuccess;
+  int epb() const { return ctx.geo.S >= 256 ? 1 : 256 / ctx.geo.S; }
+  template <class K, class... A>
+  void lp(int n, int nz, size_t smem_per_entity, K kernel, A... args) {
+    if (err != cudaSuccess || n <= 0 || nz <= 0) return;
+    const int e = epb();
+    dim3 block(ctx.geo.S, e), grid((n + e - 1) / e, 1, nz);
+    kernel<<<grid, block, smem_per_entity * e, st>>>(args...);
+    ++count;
+    err = cudaGetLastError();
+  }
+};
+
+static void diagnostics(Launcher& L, const float* u, int recompute_v) {
+  HexCtx& c = L.ctx;
+  const HexGeo& g = c.geo;
+  HexWork& w = c.w;
+  L.lp(g.nV, 1, 0, k_diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
+  L.lp(g.nC, 1, 0, k_diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
+  L.lp(g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex, (const float*)w.pv_cell, w.v, w.pv_edge,
+       recompute_v);
+}
+
+cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream) {
+  Launcher L{ctx, stream};
+  (void)s;
+  diagnostics(L, side.u, 1);
+  return L.err;
+}
+
+cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream) {
+  Launcher L{ctx, stream};
+  const HexGeo& g = ctx.geo;
+  L.lp(g.nE, 1, 0, k_recover_u, g, (const float*)s.rho, (const float*)s.rho_u, side.u);
+  L.lp(g.nC, 1, 0, k_rebuild_cell, g, (const float*)s.rho, (const float*)s.rho_theta, (const float*)s.rho_u,
+       (const float*)s.rho_w, side, ctx.w.flag);
+  return L.err;
+}
+
+cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
+                     const HexSide& side_out, cudaStream_t stream, long long* launches) {
+  Launcher L{ctx, stream};
+  const HexGeo& g = ctx.geo;
+  HexWork& w = ctx.w;
+  const int nT = ctx.n_scalars;
+  const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * 5;
+
+  if (g.moist) {
+    L.lp(g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
+    L.lp(g.nE, 1, 0, k_moist_edge, g, (const float*)in.scalars, nT, w.cqu);
+  }
+  // initial solve diagnostics with v reconstructed (rk_step=3)
+  diagnostics(L, side_in.u, 1);
+
+  const HexState* saved = &in;
+  const HexSide* s_in = &side_in;
+  for (int sub = 0; sub < ctx.split_steps; ++sub) {
+    const bool last = sub == ctx.split_steps - 1;
+    const HexState& o = last ? out : ctx.tmp[sub & 1];
+    const HexSide& so = last ? side_out : ctx.side_tmp[sub & 1];
+    // split-flux accumulation: bit 2 active, bit 0 first subcycle (copy),
+    // bit 1 last subcycle (multiply by 1/splits after the sum)
+    const int flux_mode = 4 | (sub == 0 ? 1 : 0) | (last ? 2 : 0);
+    // vertical coefficients before RK (stage-1 acoustic dts, saved theta)
+    {
+      L.lp(g.nC, 1, sm_vcoef, k_vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
+           (const float*)s_in->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
+           w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
+    }
+    L.lp(g.nE, 1, 0, k_euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
+         (const float*)w.qtot, (const float*)w.cqu, w.euler_ru);
+    L.lp(g.nC, 1, 0, k_euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
+         (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
+         w.tend_rho, w.euler_rw);
+
+    const HexState* cur = saved;
+    const HexSide* cs = s_in;
+    for (int si = 0; si < 3; ++si) {
+      const HexStage& stg = ctx.dyn[si];
+      const float dts = (float)stg.acoustic_dt;
+      if (stg.stage == 2) {
+        L.lp(g.nC, 1, sm_vcoef, k_vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
+             (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
+             w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
+      }
+      L.lp(g.nC, 1, 0, k_hdiv, g, (const float*)cur->rho_u, w.hdiv);
+      L.lp(g.nE, 1, 0, k_edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
+           w.edge_theta, w.edge_w);
+      L.lp(g.nE, 1, 0, k_tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
+           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
+      L.lp(g.nC, 1, 0, k_tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
+           (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
+           (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
+           (const float*)w.euler_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage);
+      // acoustic substeps
+      const float damp = g.smdiv_base * (1.0f / dts);
+      const float dts2 = stg.dts2;
+      for (int n = 1; n <= stg.acoustic_steps; ++n) {
+        const float* old_rt = w.rtpp[(n - 1) & 1];
+        float* new_rt = w.rtpp[n & 1];
+        if (n == 1) {
+          L.lp(g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
+               old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
+               (const float*)w.cqu, w.ru_p, w.ru_avg);
+        } else {
+          // damping of substep n-1 (new = its output, old = its input), then update n
+          const float* prev_new = w.rtpp[(n - 1) & 1];
+          const float* prev_old = w.rtpp[(n - 2) & 1];
+          L.lp(g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
+               prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
+               (const float*)w.cqu, w.ru_p, w.ru_avg);
+        }
+        L.lp(g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
+             (const float*)s_in->theta_m, (const float*)w.tend_rho, (const float*)w.tend_rt,
+             (const float*)w.tend_rw, (const float*)w.cofwr, (const float*)w.cofwz, (const float*)w.coftz,
+             (const float*)w.cofwt, (const float*)w.a_tri, (const float*)w.alpha_tri, (const float*)w.gamma_tri,
+             (const float*)cur->rho, (const float*)cs->w, (const float*)cur->rho_w, (const float*)saved->rho_w,
+             old_rt, new_rt, w.rho_pp, w.rw_p, w.ww_avg);
+      }
+      {
+        const int n = stg.acoustic_steps;
+        L.lp(g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
+             (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
+             (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
+      }
+      const float* rtpp_final = w.rtpp[stg.acoustic_steps & 1];
+      const float inv_steps = 1.0f / (float)stg.acoustic_steps;
+      const float inv_splits = 1.0f / (float)ctx.split_steps;
+      const int fm = stg.stage == 3 ? flux_mode : 0;
+      L.lp(g.nE, 1, 0, k_recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
+           (const float*)w.ru_avg, (const float*)s_in->rho_p, (const float*)w.rho_pp, o.rho_u, so.u, w.flux_u,
+           fm, inv_steps, inv_splits);
+      L.lp(g.nC, 1, 0, k_recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
+           (const float*)s_in->rtheta_p, (const float*)saved->rho_w, (const float*)w.rho_pp, rtpp_final,
+           (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
+           inv_splits, w.flag);
+      diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
+      cur = &o;
+      cs = &so;
+    }
+    saved = &o;
+    s_in = &so;
+  }
+
+  // split scalar transport: RK1, RK2 standard, RK3 monotonic FCT
+  if (nT > 0) {
+    const float* q_prev = in.scalars;
+    for (int si = 0; si < 3; ++si) {
+      const HexStage& stg = ctx.scal[si];
+      const float step = (float)stg.large_dt;
+      float* q_next = si == 2 ? out.scalars : w.q_stage[si];
+      if (si < 2 || !ctx.monotonic) {
+        const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
+        L.lp(g.nE, nT, 0, k_tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
+        L.lp(g.nC, nT, 0, k_tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
+             (const float*)out.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, q_next);
+      } else {
+        L.lp(g.nC, 1, 0, k_fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
+             (const float*)w.flux_w, w.target, w.flag);
+        L.lp(g.nE, nT, 0, k_tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
+        L.lp(g.nC, nT, 0, k_fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
+             (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
+             w.scale_in, w.scale_out, w.mass);
+        L.lp(g.nE, nT, 0, k_fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
+             (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
+        L.lp(g.nC, nT, 0, k_fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
+             (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
+             (const float*)w.target, q_next);
+      }
+      q_prev = q_next;
+    }
+  }
+  if (launches) *launches = L.count;
+  return L.err;
+}

@@ -1,0 +1,89 @@
+// Host-side context of one dycore instance (shared by the strict and fast
+// kernel builds and by the C ABI layer).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "dycore_geo.cuh"
+
+struct HexState {       // prognostic state, [entity][level] padded
+  float* rho;           // C
+  float* rho_theta;     // C
+  float* rho_u;         // E
+  float* rho_w;         // C (interfaces)
+  float* scalars;       // [T][C][S] (only the step in/out states own one)
+};
+
+struct HexSide {        // DrySavedDiagnostics
+  float* theta_m;
+  float* exner;
+  float* rho_p;
+  float* rtheta_p;
+  float* pressure_p;
+  float* u;             // E
+  float* w;             // C (interfaces)
+};
+
+struct HexWork {
+  // moist coefficients
+  float *qtot, *cqw, *cqu;
+  // diagnostics
+  float *pv_vertex, *ke_vertex, *ke, *pv_cell, *v, *pv_edge;
+  // saved Euler + stage tendencies
+  float *euler_ru, *tend_rho, *euler_rw, *hdiv, *edge_theta, *edge_w, *tend_ru, *tend_rt, *tend_rw;
+  // vertical implicit coefficients
+  float *cofwr, *cofwz, *coftz, *cofwt, *a_tri, *alpha_tri, *gamma_tri;
+  // acoustic
+  float *ru_p, *ru_avg, *rw_p, *ww_avg, *rho_pp, *rtpp[2];
+  // split mass flux (time-averaged over the dynamics subcycles)
+  float *flux_u, *flux_w;
+  // transport
+  float *q_stage[2], *edge_q, *target, *scale_in, *scale_out, *mass, *hres_lim;
+  int* flag;            // device validation flag (bit set, see HEX_FLAG_*)
+};
+
+struct HexStage {
+  int stage;            // 1..3
+  double large_dt;
+  double acoustic_dt;
+  int acoustic_steps;
+  float dts2;           // FP32 dts^2 used by the implicit solve
+};
+
+struct HexCtx {
+  int numerics;         // 0 strict, 1 fast
+  int n_scalars;
+  double dt;
+  int split_steps;
+  int monotonic;
+  HexGeo geo;
+  HexStage dyn[3];      // dynamics subcycle schedule
+  HexStage scal[3];     // scalar transport schedule
+  HexState in, out, tmp[2];
+  HexSide side_in, side_out, side_tmp[2];
+  HexWork w;
+  std::vector<void*> allocations;
+  size_t device_bytes = 0;
+  cudaStream_t bound_stream = nullptr;
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  int parity = 0;       // 0: state in `in`, 1: state in `out`
+  long long steps_done = 0;
+  long long launches_per_step = 0;
+};
+
+namespace hexdyn_strict {
+cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
+                     const HexSide& side_out, cudaStream_t stream, long long* launches);
+cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
+cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
+}  // namespace hexdyn_strict
+namespace hexdyn_fast {
+cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
+                     const HexSide& side_out, cudaStream_t stream, long long* launches);
+cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
+cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
+}  // namespace hexdyn_fast

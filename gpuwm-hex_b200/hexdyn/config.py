@@ -1,0 +1,161 @@
+"""Dycore configuration with refusal-based validation.
+
+Mirrors the knobs of the reference's ``V841DryDycoreConfig``
+(``hexcore/config_v841.py:114``, defaults ``:117-140``, base validation
+``hexcore/driver.py:232-501``) that the GPU step path reads.  A value outside
+what this path implements is refused by name, before any launch, with the
+same ``ConfigurationRefusal(knob, value, reason, declaration)`` shape as
+``hexcore/errors.py:17``.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, fields
+from typing import Any, Mapping
+
+
+class ConfigurationRefusal(RuntimeError):
+    """A requested configuration knob has no implementation on this path."""
+
+    def __init__(self, knob: str, value: object, reason: str, declaration: str) -> None:
+        self.knob = knob
+        self.value = value
+        self.reason = reason
+        self.declaration = declaration
+        super().__init__(f"{knob}={value!r} is refused: {reason}. To run, declare {declaration}.")
+
+
+def _refuse(knob: str, value: object, reason: str, declaration: str) -> None:
+    raise ConfigurationRefusal(knob, value, reason, declaration)
+
+
+@dataclass(frozen=True)
+class DycoreConfig:
+    """The v8.4.1/8.4.2 dry-plus-tracer lane on one GPU."""
+
+    config_dt: float = 30.0
+    config_time_integration_order: int = 3
+    config_number_of_sub_steps: int = 2
+    config_dynamics_split_steps: int = 3
+    config_split_dynamics_transport: bool = True
+    config_scalar_advection: bool = True
+    config_monotonic: bool = True
+    config_positive_definite: bool = False
+    config_scalar_adv_order: int = 3
+    config_scalar_vadv_order: int = 3
+    config_coef_3rd_order: float = 0.25
+    config_apvm_upwinding: float = 0.5
+    config_epssm: float = 0.0
+    config_epssm_minimum: float = 0.1
+    config_epssm_maximum: float = 0.5
+    config_epssm_transition_bottom_z: float = 30_000.0
+    config_epssm_transition_top_z: float = 50_000.0
+    config_divergence_damping: bool = True
+    config_smdiv: float = 0.1
+    config_len_disp: float = 0.0
+    config_xnutr: float = 0.0
+    config_horiz_mixing: str = "off"
+    config_moist_physics: bool = False
+    config_rayleigh_damp_u: bool = False
+    config_apply_lbcs: bool = False
+    # Coefficient semantics of the carried scalars: "native" applies
+    # atm_compute_moist_coefficients from every scalar each step (native MPAS
+    # and the reference CUDA driver with physics off); "dry" keeps qtot=0,
+    # cqu=cqw=1 (the reference CPU driver on a global mesh).
+    moist_coefficients: str = "native"
+    # "strict": bit-identical to the reference authority; "fast": FMA.
+    numerics: str = "strict"
+
+    @classmethod
+    def from_mapping(cls, raw: Mapping[str, Any]) -> "DycoreConfig":
+        known = {f.name for f in fields(cls)}
+        unknown = sorted(set(raw) - known)
+        if unknown:
+            _refuse(unknown[0], raw[unknown[0]], "this option is not implemented on the GPU step path",
+                    f"a supported value after porting {unknown[0]!r}")
+        out = cls(**raw)
+        out.validate()
+        return out
+
+    @classmethod
+    def from_reference(cls, config: Any, **overrides: Any) -> "DycoreConfig":
+        """Project a reference ``V841DryDycoreConfig`` (or any object with the
+        same attribute names) onto this configuration."""
+        values = {f.name: getattr(config, f.name) for f in fields(cls) if hasattr(config, f.name)}
+        values.update(overrides)
+        out = cls(**values)
+        out.validate()
+        return out
+
+    def validate(self) -> None:
+        if not math.isfinite(self.config_dt) or self.config_dt <= 0.0:
+            _refuse("config_dt", self.config_dt, "the timestep must be finite and positive", "config_dt>0")
+        if self.config_time_integration_order != 3:
+            _refuse("config_time_integration_order", self.config_time_integration_order,
+                    "the GPU path implements the RK3 schedule only", "config_time_integration_order=3")
+        if not isinstance(self.config_number_of_sub_steps, int) or self.config_number_of_sub_steps < 1:
+            _refuse("config_number_of_sub_steps", self.config_number_of_sub_steps,
+                    "the split-explicit acoustic loop requires a positive count", "config_number_of_sub_steps>=1")
+        if self.config_dynamics_split_steps not in (1, 3):
+            _refuse("config_dynamics_split_steps", self.config_dynamics_split_steps,
+                    "the drivers implement one and three dynamics subcycles only",
+                    "config_dynamics_split_steps=1 or 3")
+        if not self.config_split_dynamics_transport:
+            _refuse("config_split_dynamics_transport", False,
+                    "the GPU path transports scalars after the dynamics subcycles (split transport)",
+                    "config_split_dynamics_transport=True")
+        if not self.config_scalar_advection:
+            _refuse("config_scalar_advection", False, "scalar advection is always active on this path",
+                    "config_scalar_advection=True")
+        if self.config_scalar_adv_order != 3 or self.config_scalar_vadv_order != 3:
+            _refuse("config_scalar_adv_order", (self.config_scalar_adv_order, self.config_scalar_vadv_order),
+                    "the path uses the third-order horizontal and vertical fluxes",
+                    "config_scalar_adv_order=3 and config_scalar_vadv_order=3")
+        if not math.isfinite(self.config_coef_3rd_order) or self.config_coef_3rd_order < 0.0:
+            _refuse("config_coef_3rd_order", self.config_coef_3rd_order,
+                    "the upwind coefficient must be finite and non-negative", "config_coef_3rd_order=0.25")
+        if not math.isfinite(self.config_apvm_upwinding) or self.config_apvm_upwinding < 0.0:
+            _refuse("config_apvm_upwinding", self.config_apvm_upwinding,
+                    "the APVM branch requires a finite non-negative coefficient", "config_apvm_upwinding>=0")
+        if not math.isfinite(self.config_smdiv) or self.config_smdiv < 0.0:
+            _refuse("config_smdiv", self.config_smdiv, "the divergence damping coefficient is non-negative",
+                    "config_smdiv>=0")
+        if self.config_divergence_damping and self.config_smdiv == 0.0:
+            _refuse("config_smdiv", 0.0, "the enabled divergence-damping branch would be an accidental no-op",
+                    "config_smdiv>0 when config_divergence_damping=True")
+        if not self.config_divergence_damping and self.config_smdiv != 0.0:
+            _refuse("config_divergence_damping", False, "a nonzero config_smdiv must not be silently ignored",
+                    "config_divergence_damping=True when config_smdiv>0")
+        if self.config_len_disp < 0.0 or not math.isfinite(self.config_len_disp):
+            _refuse("config_len_disp", self.config_len_disp, "a negative filter length is not admitted",
+                    "config_len_disp>=0 (zero selects nominalMinDc)")
+        mn, mx = self.config_epssm_minimum, self.config_epssm_maximum
+        lo, hi = self.config_epssm_transition_bottom_z, self.config_epssm_transition_top_z
+        if not (0.0 <= mn <= 1.0) or not (mn <= mx <= 1.0):
+            _refuse("config_epssm_minimum", (mn, mx), "the off-centering profile must be ordered in [0,1]",
+                    "0<=config_epssm_minimum<=config_epssm_maximum<=1")
+        if not (lo >= 0.0 and hi > lo):
+            _refuse("config_epssm_transition_top_z", (lo, hi), "the transition must have positive width",
+                    "0<=bottom<top")
+        if self.config_xnutr != 0.0:
+            _refuse("config_xnutr", self.config_xnutr, "implicit upper-level w damping is not on this path yet",
+                    "config_xnutr=0.0")
+        if self.config_horiz_mixing not in ("off", "2d_fixed"):
+            _refuse("config_horiz_mixing", self.config_horiz_mixing,
+                    "Smagorinsky mixing is outside this path (mixing is off in its configurations)",
+                    "config_horiz_mixing='off'")
+        for knob in ("config_moist_physics", "config_rayleigh_damp_u", "config_apply_lbcs"):
+            if getattr(self, knob):
+                _refuse(knob, True, "physics, upper damping and limited-area branches are outside this path",
+                        f"{knob}=False")
+        if self.moist_coefficients not in ("native", "dry"):
+            _refuse("moist_coefficients", self.moist_coefficients, "unknown coefficient semantics",
+                    "moist_coefficients='native' or 'dry'")
+        if self.numerics not in ("strict", "fast"):
+            _refuse("numerics", self.numerics, "unknown numerics mode", "numerics='strict' or 'fast'")
+
+    @property
+    def fct(self) -> bool:
+        """RK3 stage uses the monotonic/positive-definite limiter (transport.py:2210)."""
+        return bool(self.config_monotonic or self.config_positive_definite)

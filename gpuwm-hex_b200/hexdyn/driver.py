@@ -1,0 +1,391 @@
+"""Host driver with the reference's dycore step interface.
+
+``HexDycoreDriver`` presents the methods of the reference's
+``CudaDryDycoreDriver`` (``hexcore/cuda_driver.py:2658``):
+
+* ``from_host(mesh, state, vertical, reference, config, *, saved_diagnostics,
+  terrain_metrics, advection_coefficients, reference_wind_profiles)``
+  (``:2826``) uploads once and owns the device copies;
+* ``step_device()`` (``:5751``) advances one large step on the device and
+  returns a ``DeviceStepResult`` whose ``atmosphere`` exposes the new state as
+  torch CUDA tensors (zero copy);
+* ``step()`` (``:6112``) is ``step_device()`` plus the download of the state
+  and the saved diagnostics.
+
+Arguments are duck-typed on the reference's attribute names
+(``PrognosticState``, ``VerticalGrid``, ``DryReferenceState``,
+``TerrainMetrics``, ``AdvectionCoefficients``, ``V841ReferenceWindProfiles``,
+``DrySavedDiagnostics``), so the reference's own objects can be passed.  All
+arithmetic runs in the CUDA library behind the C ABI (include/hexdyn.h);
+there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import _lib
+from .config import ConfigurationRefusal, DycoreConfig
+
+F32 = np.float32
+
+
+def mesh_array(mesh: Any, name: str) -> np.ndarray:
+    """``_mesh_array`` of the reference: attribute first, then ``mesh.arrays``."""
+    try:
+        return np.asarray(getattr(mesh, name))
+    except AttributeError:
+        arrays = getattr(mesh, "arrays", None)
+        if arrays is None or name not in arrays:
+            raise AttributeError(f"mesh has no MPAS field {name!r}") from None
+        return np.asarray(arrays[name])
+
+
+def _schedule_dts(cfg: DycoreConfig) -> list[float]:
+    dt_dyn = cfg.config_dt / cfg.config_dynamics_split_steps
+    n = cfg.config_number_of_sub_steps
+    return [dt_dyn / 3.0, dt_dyn / n, dt_dyn / n]
+
+
+@dataclass
+class HostState:
+    rho: np.ndarray
+    rho_theta: np.ndarray
+    rho_u: np.ndarray
+    rho_w: np.ndarray
+    scalars: np.ndarray
+    time_seconds: float = 0.0
+
+
+@dataclass
+class HostSidecar:
+    theta_m: np.ndarray
+    exner: np.ndarray
+    density_perturbation: np.ndarray
+    rho_theta_perturbation: np.ndarray
+    pressure_perturbation: np.ndarray
+    normal_velocity: np.ndarray
+    vertical_velocity: np.ndarray
+
+
+class _CudaArray:
+    """``__cuda_array_interface__`` view of library-owned device memory."""
+
+    def __init__(self, ptr: int, shape: tuple[int, ...], owner: Any):
+        self._owner = owner
+        self.__cuda_array_interface__ = {
+            "shape": shape, "typestr": "<f4", "data": (int(ptr), False), "version": 3, "strides": None,
+        }
+
+
+@dataclass
+class DeviceAtmosphere:
+    """Device views of the current state: each field is a torch tensor in the
+    library's padded [entity][level] layout (``padded``) and as a logical
+    [level][entity] view (``logical``)."""
+
+    driver: "HexDycoreDriver"
+
+    def padded(self, name: str):
+        import torch
+
+        ptr = C.c_void_p()
+        _lib.check(self.driver._lib.hexdyn_device_field(self.driver._handle, _lib.FIELDS[name], C.byref(ptr)))
+        n, blocks = self.driver._entities(name)
+        shape = (blocks * n, self.driver.level_stride) if blocks > 1 else (n, self.driver.level_stride)
+        return torch.as_tensor(_CudaArray(ptr.value, shape, self.driver), device="cuda")
+
+    def logical(self, name: str):
+        rows = self.driver._rows(name)
+        t = self.padded(name)[:, :rows]
+        n, blocks = self.driver._entities(name)
+        if blocks > 1:
+            return t.reshape(blocks, n, rows).transpose(1, 2)
+        return t.t()
+
+
+@dataclass
+class StepReceipt:
+    steps: int
+    flag: int
+    launches_per_step: int
+    device_bytes: int
+    graph: bool
+
+
+@dataclass
+class DeviceStepResult:
+    atmosphere: DeviceAtmosphere
+    receipt: StepReceipt
+
+
+@dataclass
+class HostStepResult:
+    state: HostState
+    saved_diagnostics: HostSidecar
+    receipt: StepReceipt
+
+
+class HexDycoreDriver:
+    """One dycore instance resident on the current CUDA device."""
+
+    def __init__(self, handle: C.c_void_p, keep: dict, cfg: DycoreConfig, sizes: dict, stream: Any):
+        self._lib = _lib.load()
+        self._handle = handle
+        self._keep = keep
+        self.config = cfg
+        self.sizes = sizes
+        self._stream = stream
+        self.level_stride = int(self._lib.hexdyn_level_stride(handle))
+        self.time_seconds = 0.0
+        self._graph = False
+
+    # ------------------------------------------------------------ creation
+    @classmethod
+    def from_host(cls, mesh: Any, state: Any, vertical: Any, reference: Any, config: Any, *,
+                  saved_diagnostics: Any = None, terrain_metrics: Any = None,
+                  advection_coefficients: Any = None, reference_wind_profiles: Any = None,
+                  stream: Any = None, capture_graph: bool = False, **config_overrides: Any) -> "HexDycoreDriver":
+        cfg = config if isinstance(config, DycoreConfig) else DycoreConfig.from_reference(config, **config_overrides)
+        if config_overrides and isinstance(config, DycoreConfig):
+            cfg = DycoreConfig(**{**cfg.__dict__, **config_overrides})
+            cfg.validate()
+        if terrain_metrics is None:
+            _refuse_missing("zb", "terrain_metrics=TerrainMetrics(zb_cell, zb3_cell)")
+        if advection_coefficients is None:
+            _refuse_missing("adv_coefs", "advection_coefficients=AdvectionCoefficients(...)")
+        if reference_wind_profiles is None:
+            _refuse_missing("u_init", "reference_wind_profiles=V841ReferenceWindProfiles(u_init, v_init)")
+        lib = _lib.load()
+        desc, keep, sizes = _build_descriptor(mesh, state, vertical, reference, cfg, terrain_metrics,
+                                              advection_coefficients, reference_wind_profiles)
+        handle = C.c_void_p()
+        _lib.check(lib.hexdyn_create(C.byref(desc), C.byref(handle)))
+        drv = cls(handle, keep, cfg, sizes, stream)
+        drv.set_state(state, saved_diagnostics)
+        if capture_graph:
+            drv.capture_graph()
+        return drv
+
+    # ----------------------------------------------------------- plumbing
+    def _stream_handle(self):
+        if self._stream is not None:
+            return C.c_void_p(int(getattr(self._stream, "cuda_stream", self._stream)))
+        try:
+            import torch
+
+            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:  # noqa: BLE001 - no torch: the legacy default stream
+            return C.c_void_p(0)
+
+    def _entities(self, name: str) -> tuple[int, int]:
+        s = self.sizes
+        if name in ("rho_u", "normal_velocity"):
+            return s["n_edges"], 1
+        if name == "scalars":
+            return s["n_cells"], s["n_scalars"]
+        return s["n_cells"], 1
+
+    def _rows(self, name: str) -> int:
+        L = self.sizes["n_levels"]
+        return L + 1 if name in ("rho_w", "vertical_velocity") else L
+
+    def _shape(self, name: str) -> tuple[int, ...]:
+        n, blocks = self._entities(name)
+        rows = self._rows(name)
+        return (blocks, rows, n) if name == "scalars" else (rows, n)
+
+    def _put(self, name: str, value: Any, stream) -> None:
+        arr = np.ascontiguousarray(value, dtype=F32)
+        if arr.shape != self._shape(name):
+            raise ValueError(f"{name} shape {arr.shape} != {self._shape(name)}")
+        self._keep.setdefault("_uploads", []).append(arr)
+        _lib.check(self._lib.hexdyn_set_state(self._handle, _lib.FIELDS[name],
+                                              arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, stream))
+
+    def set_state(self, state: Any, saved_diagnostics: Any = None) -> None:
+        """Upload a prognostic state (and sidecar, else rebuild it on the device
+        exactly as ``hexcore/driver.py:2655`` does)."""
+        stream = self._stream_handle()
+        self._keep["_uploads"] = []
+        for name in _lib.STATE_FIELDS:
+            if name == "scalars" and self.sizes["n_scalars"] == 0:
+                continue
+            self._put(name, getattr(state, name), stream)
+        if saved_diagnostics is None:
+            _lib.check(self._lib.hexdyn_rebuild_sidecar(self._handle, stream))
+        else:
+            for name in _lib.SIDECAR_FIELDS:
+                self._put(name, getattr(saved_diagnostics, name), stream)
+        self.time_seconds = float(getattr(state, "time_seconds", 0.0))
+        self.synchronize()
+        self._keep["_uploads"] = []
+
+    def synchronize(self) -> None:
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+
+    def capture_graph(self) -> None:
+        """Capture the whole RK3 large step as CUDA graphs (one per buffer parity)."""
+        _lib.check(self._lib.hexdyn_capture_graph(self._handle, self._stream_handle()))
+        self._graph = True
+
+    # -------------------------------------------------------------- steps
+    def step_async(self, nsteps: int = 1) -> None:
+        _lib.check(self._lib.hexdyn_step_async(self._handle, self._stream_handle(), int(nsteps)))
+        self.time_seconds += nsteps * self.config.config_dt
+
+    def read_flag(self) -> int:
+        flag = C.c_int(0)
+        rc = self._lib.hexdyn_read_flag(self._handle, self._stream_handle(), C.byref(flag))
+        if rc == _lib.HEXDYN_E_NUMERIC:
+            raise FloatingPointError(_lib.last_error())
+        _lib.check(rc)
+        return flag.value
+
+    def step_device(self, nsteps: int = 1) -> DeviceStepResult:
+        flag = C.c_int(0)
+        done = C.c_int(0)
+        rc = self._lib.hexdyn_step(self._handle, self._stream_handle(), int(nsteps), C.byref(flag), C.byref(done))
+        if rc == _lib.HEXDYN_E_NUMERIC:
+            raise FloatingPointError(_lib.last_error())
+        _lib.check(rc)
+        self.time_seconds += nsteps * self.config.config_dt
+        return DeviceStepResult(DeviceAtmosphere(self), self.receipt(nsteps, flag.value))
+
+    def receipt(self, steps: int = 0, flag: int = 0) -> StepReceipt:
+        return StepReceipt(steps=steps, flag=flag,
+                           launches_per_step=int(self._lib.hexdyn_launches_per_step(self._handle)),
+                           device_bytes=int(self._lib.hexdyn_device_bytes(self._handle)), graph=self._graph)
+
+    def get_state(self, stream=None) -> tuple[HostState, HostSidecar]:
+        st = self._stream_handle() if stream is None else stream
+        out = {}
+        for name in (*_lib.STATE_FIELDS, *_lib.SIDECAR_FIELDS):
+            shape = self._shape(name)
+            arr = np.empty(shape, dtype=F32)
+            if arr.size:
+                _lib.check(self._lib.hexdyn_get_state(self._handle, _lib.FIELDS[name],
+                                                      arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, st))
+            out[name] = arr
+        self.synchronize()
+        state = HostState(**{k: out[k] for k in _lib.STATE_FIELDS}, time_seconds=self.time_seconds)
+        side = HostSidecar(**{k: out[k] for k in _lib.SIDECAR_FIELDS})
+        return state, side
+
+    def step(self, nsteps: int = 1) -> HostStepResult:
+        res = self.step_device(nsteps)
+        state, side = self.get_state()
+        return HostStepResult(state, side, res.receipt)
+
+    def close(self) -> None:
+        if self._handle:
+            self._lib.hexdyn_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def _refuse_missing(knob: str, declaration: str) -> None:
+    raise ConfigurationRefusal(knob, None, "the v8.4.1 step needs this input", declaration)
+
+
+def _i32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x), dtype=np.int32)
+
+
+def _f32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x).astype(F32, copy=False))
+
+
+def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terrain, adv, winds):
+    ncells = int(mesh_array(mesh, "areaCell").size)
+    nedges = int(mesh_array(mesh, "dcEdge").size)
+    nvert = int(mesh_array(mesh, "areaTriangle").size)
+    nlev = int(np.asarray(vertical.zz).shape[0])
+    scalars = np.asarray(state.scalars)
+    keep: dict[str, np.ndarray] = {}
+    eoc = _i32(mesh_array(mesh, "edgesOnCell"))
+    eoe = _i32(mesh_array(mesh, "edgesOnEdge"))
+    adv_cells = _i32(adv.adv_cells_for_edge)
+    angle = np.asarray(mesh_array(mesh, "angleEdge")).astype(F32)
+    # cos/sin of the FP32 angle with NumPy's scalar kernel, as the reference
+    # evaluates them (hexcore/dynamics_v841.py:163-165).
+    cos_a = np.asarray([np.cos(a) for a in angle], dtype=F32)
+    sin_a = np.asarray([np.sin(a) for a in angle], dtype=F32)
+    arrays = {
+        "cells_on_edge": _i32(mesh_array(mesh, "cellsOnEdge")),
+        "edges_on_cell": eoc,
+        "cells_on_cell": _i32(mesh_array(mesh, "cellsOnCell"))[:, : eoc.shape[1]].copy(),
+        "vertices_on_cell": _i32(mesh_array(mesh, "verticesOnCell"))[:, : eoc.shape[1]].copy(),
+        "n_edges_on_cell": _i32(mesh_array(mesh, "nEdgesOnCell")),
+        "vertices_on_edge": _i32(mesh_array(mesh, "verticesOnEdge")),
+        "edges_on_vertex": _i32(mesh_array(mesh, "edgesOnVertex")),
+        "cells_on_vertex": _i32(mesh_array(mesh, "cellsOnVertex")),
+        "edges_on_edge": eoe,
+        "n_edges_on_edge": _i32(mesh_array(mesh, "nEdgesOnEdge")),
+        "adv_cells": adv_cells,
+        "n_adv_cells": _i32(adv.n_adv_cells_for_edge),
+        "dc_edge": _f32(mesh_array(mesh, "dcEdge")),
+        "dv_edge": _f32(mesh_array(mesh, "dvEdge")),
+        "area_cell": _f32(mesh_array(mesh, "areaCell")),
+        "area_triangle": _f32(mesh_array(mesh, "areaTriangle")),
+        "kite_areas": _f32(mesh_array(mesh, "kiteAreasOnVertex")),
+        "weights_on_edge": _f32(mesh_array(mesh, "weightsOnEdge")),
+        "f_vertex": _f32(mesh_array(mesh, "fVertex")),
+        "f_edge": _f32(mesh_array(mesh, "fEdge")),
+        "cos_angle_edge": cos_a,
+        "sin_angle_edge": sin_a,
+        "adv_coefs": _f32(adv.adv_coefs),
+        "adv_coefs_3rd": _f32(adv.adv_coefs_3rd),
+        "fzm": _f32(vertical.fzm), "fzp": _f32(vertical.fzp),
+        "rdzw": _f32(vertical.rdzw), "rdzu": _f32(vertical.rdzu),
+        "zz": _f32(vertical.zz), "zxu": _f32(vertical.zxu),
+        "dss": np.zeros((nlev, ncells), dtype=F32),
+        "zb_cell": _f32(terrain.zb_cell), "zb3_cell": _f32(terrain.zb3_cell),
+        "rho_base": _f32(reference.rho_base), "rho_theta_base": _f32(reference.rho_theta_base),
+        "exner_base": _f32(reference.exner_base),
+        "u_init": _f32(winds.u_init), "v_init": _f32(winds.v_init),
+    }
+    desc = _lib.HexDynDesc()
+    for name, arr in arrays.items():
+        keep[name] = arr
+        ptype = C.POINTER(C.c_int32) if arr.dtype == np.int32 else C.POINTER(C.c_float)
+        setattr(desc, name, arr.ctypes.data_as(ptype))
+    desc.n_cells, desc.n_edges, desc.n_vertices, desc.n_levels = ncells, nedges, nvert, nlev
+    desc.max_edges = eoc.shape[1]
+    desc.max_edges2 = eoe.shape[1]
+    desc.adv_width = adv_cells.shape[1]
+    desc.n_scalars = int(scalars.shape[0])
+    desc.cf1, desc.cf2, desc.cf3 = float(vertical.cf1), float(vertical.cf2), float(vertical.cf3)
+    nominal = np.asarray(mesh_array(mesh, "nominalMinDc")).reshape(-1)
+    desc.nominal_min_dc = float(F32(float(nominal[0])))
+    desc.dt = float(cfg.config_dt)
+    desc.n_sub_steps = cfg.config_number_of_sub_steps
+    desc.split_steps = cfg.config_dynamics_split_steps
+    desc.monotonic = 1 if cfg.fct else 0
+    desc.moist = 1 if cfg.moist_coefficients == "native" else 0
+    desc.numerics = 1 if cfg.numerics == "fast" else 0
+    desc.coef_3rd_order = cfg.config_coef_3rd_order
+    desc.apvm_upwinding = cfg.config_apvm_upwinding
+    desc.smdiv = cfg.config_smdiv
+    desc.len_disp = cfg.config_len_disp
+    desc.epssm_minimum = cfg.config_epssm_minimum
+    desc.epssm_maximum = cfg.config_epssm_maximum
+    desc.epssm_bottom_z = cfg.config_epssm_transition_bottom_z
+    desc.epssm_top_z = cfg.config_epssm_transition_top_z
+    desc.rgas, desc.cp, desc.gravity, desc.p0 = 287.0, 1004.5, 9.80616, 100000.0
+    for i, dts in enumerate(_schedule_dts(cfg)):
+        desc.acoustic_dts2[i] = float(F32(dts) ** 2)
+    sizes = dict(n_cells=ncells, n_edges=nedges, n_vertices=nvert, n_levels=nlev, n_scalars=int(scalars.shape[0]))
+    return desc, keep, sizes

@@ -1,0 +1,174 @@
+/*
+ * hexdyn: B200-native MPAS-A v8.4.2 dry-plus-tracer dycore step, C ABI.
+ *
+ * The entry points are the drop-in boundary for the reference's dycore step
+ * path (gpuwm-hex 0.5.0, tree/src/hexcore/).  Each declaration names the
+ * reference interface it replaces:
+ *
+ *   hexdyn_abi_version      <- hexcore/native/step_submit.c:33 hex_step_abi_version
+ *   hexdyn_create           <- hexcore/cuda_driver.py:2826 CudaDryDycoreDriver.from_host
+ *                              (upload of mesh, vertical grid, reference state,
+ *                              terrain and advection coefficients; validation
+ *                              as in hexcore/cuda_driver.py:3096 _validate_config)
+ *   hexdyn_set_state        <- from_host's DeviceAtmosphere upload
+ *                              (hexcore/cuda_backend/containers.py:1098)
+ *   hexdyn_get_state        <- hexcore/cuda_driver.py:6112 step() host download
+ *   hexdyn_step             <- hexcore/cuda_driver.py:5751 step_device /
+ *                              :4854 _step_device_v841 (flag read :5355-5402)
+ *   hexdyn_capture_graph    <- hexcore/cuda_subcycle_graphs.py:64 attach_subcycle_graphs
+ *                              (here the whole large step is one graph)
+ *   hexdyn_last_error       <- the refusal / FloatingPointError text of the driver
+ *   hexdyn_destroy          <- driver teardown
+ *
+ * Conventions (hexcore/native/step_submit.c:33-90): every call returns an
+ * int status, 0 on success, a negative HEXDYN_E_* code for a refused
+ * argument, or a positive CUDA error code; nothing is retried.  Host arrays
+ * use the reference's logical layout: [level][entity] for fields, row-major
+ * [entity][slot] for connectivity, zero-based indices, int32 and float32.
+ * One handle is bound to one stream at a time and steps one state at a time.
+ */
+#ifndef HEXDYN_H
+#define HEXDYN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HEXDYN_ABI_VERSION 1
+
+#define HEXDYN_OK 0
+#define HEXDYN_E_ARG (-1)        /* invalid argument or descriptor */
+#define HEXDYN_E_STATE (-2)      /* call out of order (no state bound, ...) */
+#define HEXDYN_E_NUMERIC (-3)    /* device validation flag set (see flag_out) */
+#define HEXDYN_E_CAPACITY (-4)   /* size beyond a stated maximum */
+
+/* Validation-flag bits reported by hexdyn_step (hexcore/cuda_driver.py:4885). */
+#define HEXDYN_FLAG_DENSITY 1    /* rho or rho_theta became non-positive */
+#define HEXDYN_FLAG_SINGULAR 2   /* singular vertical acoustic system */
+#define HEXDYN_FLAG_POWF 4       /* Exner argument outside positive normals */
+#define HEXDYN_FLAG_TARGET 8     /* non-positive FCT target density */
+
+/* Field identifiers for hexdyn_set_state / hexdyn_get_state. */
+enum HexDynField {
+  HEXDYN_RHO = 0,             /* rho_zz      [L][C]   */
+  HEXDYN_RHO_THETA = 1,       /* rho_theta_m [L][C]   */
+  HEXDYN_RHO_U = 2,           /* ru          [L][E]   */
+  HEXDYN_RHO_W = 3,           /* rw          [L+1][C] */
+  HEXDYN_SCALARS = 4,         /* scalars     [T][L][C] */
+  HEXDYN_THETA_M = 5,         /* saved diagnostics (DrySavedDiagnostics) */
+  HEXDYN_EXNER = 6,
+  HEXDYN_RHO_P = 7,
+  HEXDYN_RHO_THETA_P = 8,
+  HEXDYN_PRESSURE_P = 9,
+  HEXDYN_U = 10,              /* [L][E]   */
+  HEXDYN_W = 11,              /* [L+1][C] */
+  HEXDYN_NUM_FIELDS = 12
+};
+
+typedef struct HexDynDesc {
+  /* sizes */
+  int32_t n_cells, n_edges, n_vertices, n_levels;
+  int32_t max_edges, max_edges2, adv_width, n_scalars;
+  /* connectivity */
+  const int32_t* cells_on_edge;     /* [E][2] */
+  const int32_t* edges_on_cell;     /* [C][max_edges] */
+  const int32_t* cells_on_cell;     /* [C][max_edges] */
+  const int32_t* vertices_on_cell;  /* [C][max_edges] */
+  const int32_t* n_edges_on_cell;   /* [C] */
+  const int32_t* vertices_on_edge;  /* [E][2] */
+  const int32_t* edges_on_vertex;   /* [V][3] */
+  const int32_t* cells_on_vertex;   /* [V][3] */
+  const int32_t* edges_on_edge;     /* [E][max_edges2] */
+  const int32_t* n_edges_on_edge;   /* [E] */
+  const int32_t* adv_cells;         /* [E][adv_width] advCellsForEdge */
+  const int32_t* n_adv_cells;       /* [E] */
+  /* FP32 geometry (the float64 static fields rounded to float32) */
+  const float *dc_edge, *dv_edge, *area_cell, *area_triangle;
+  const float* kite_areas;          /* [V][3] */
+  const float* weights_on_edge;     /* [E][max_edges2] */
+  const float *f_vertex, *f_edge;
+  const float *cos_angle_edge, *sin_angle_edge; /* cos/sin of FP32 angleEdge */
+  const float *adv_coefs, *adv_coefs_3rd;       /* [E][adv_width] */
+  /* vertical grid */
+  const float *fzm, *fzp, *rdzw, *rdzu;         /* [L] */
+  const float* zz;                  /* [L][C] */
+  const float* zxu;                 /* [L][E] */
+  const float* dss;                 /* [L][C] implicit w damping */
+  const float* zb_cell;             /* [L+1][C][max_edges] */
+  const float* zb3_cell;            /* [L+1][C][max_edges], x coef_3rd_order */
+  const float *rho_base, *rho_theta_base, *exner_base; /* [L][C] */
+  const float *u_init, *v_init;     /* [L] */
+  float cf1, cf2, cf3;
+  float nominal_min_dc;
+  /* configuration (V841DryDycoreConfig, hexcore/config_v841.py:114) */
+  double dt;
+  int32_t n_sub_steps;              /* config_number_of_sub_steps */
+  int32_t split_steps;              /* config_dynamics_split_steps (1 or 3) */
+  int32_t monotonic;                /* config_monotonic */
+  int32_t moist;                    /* 0: dry coefficients, 1: native (all scalars load) */
+  int32_t numerics;                 /* 0: strict (bitwise), 1: fast (FMA) */
+  float coef_3rd_order, apvm_upwinding, smdiv, len_disp;
+  float epssm_minimum, epssm_maximum, epssm_bottom_z, epssm_top_z;
+  float rgas, cp, gravity, p0;
+  /* dts^2 of the three dynamics RK stages as the host computes FP32
+   * dts**2 (NumPy's scalar power, which is powf and not always dts*dts);
+   * zero selects dts*dts. */
+  float acoustic_dts2[3];
+} HexDynDesc;
+
+typedef struct HexDynHandle HexDynHandle;
+
+int hexdyn_abi_version(void);
+
+/* Validate the descriptor, allocate device memory, upload the static
+ * fields.  Runs on the current CUDA device. */
+int hexdyn_create(const HexDynDesc* desc, HexDynHandle** out);
+
+/* Upload one field of the current state from host memory (logical layout),
+ * enqueued on `stream` (asynchronous when `host` is pinned; the caller must
+ * keep `host` alive until the stream reaches the copy). */
+int hexdyn_set_state(HexDynHandle* h, int field, const float* host, size_t count, void* stream);
+
+/* Rebuild the saved diagnostics from the current prognostic state, as the
+ * reference does when no sidecar is supplied (hexcore/driver.py:2655). */
+int hexdyn_rebuild_sidecar(HexDynHandle* h, void* stream);
+
+/* Download one field of the current state into host memory, enqueued on
+ * `stream` (synchronise the stream before reading `host`). */
+int hexdyn_get_state(HexDynHandle* h, int field, float* host, size_t count, void* stream);
+
+/* Advance nsteps large steps on `stream` (a cudaStream_t; NULL = default).
+ * Reads the validation flag once at the end; *flag_out receives it and a
+ * non-zero flag returns HEXDYN_E_NUMERIC.  *completed counts the steps
+ * enqueued. */
+int hexdyn_step(HexDynHandle* h, void* stream, int nsteps, int* flag_out, int* completed);
+
+/* Enqueue nsteps large steps without reading the flag (asynchronous). */
+int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps);
+
+/* Read and clear the validation flag (synchronises `stream`). */
+int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out);
+
+/* Capture the whole large step into CUDA graphs (one per buffer parity);
+ * later hexdyn_step calls replay them. */
+int hexdyn_capture_graph(HexDynHandle* h, void* stream);
+
+/* Device pointer of a field of the current state ([entity][level] padded
+ * layout, level stride from hexdyn_level_stride) for zero-copy consumers. */
+int hexdyn_device_field(HexDynHandle* h, int field, void** dev_ptr);
+int hexdyn_level_stride(HexDynHandle* h);
+long long hexdyn_launches_per_step(HexDynHandle* h);
+size_t hexdyn_device_bytes(HexDynHandle* h);
+
+/* Copy the last error message of this thread into buf. */
+int hexdyn_last_error(char* buf, size_t len);
+
+int hexdyn_destroy(HexDynHandle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEXDYN_H */

@@ -1,0 +1,50 @@
+"""Shared test helpers: golden fixtures and synthetic cases as driver inputs."""
+
+from __future__ import annotations
+
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+from hexdyn.case import VerticalGridData
+from hexdyn.mesh import VoronoiMesh
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+STATE = ("rho", "rho_theta", "rho_u", "rho_w", "scalars")
+SIDE = ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
+        "pressure_perturbation", "normal_velocity", "vertical_velocity")
+
+
+def load_golden(name: str) -> dict:
+    with np.load(GOLDEN / f"step_{name}.npz", allow_pickle=False) as z:
+        return {k: z[k] for k in z.files}
+
+
+def inputs(fx: dict) -> dict:
+    """The case arrays (``hexdyn.case.case_arrays`` layout) of a fixture."""
+    return {k[3:]: v for k, v in fx.items() if k.startswith("in.")}
+
+
+def case_from_arrays(arr: dict) -> SimpleNamespace:
+    """A duck-typed case (reference attribute names) from case arrays."""
+    mesh = VoronoiMesh(arrays={k[5:]: v for k, v in arr.items() if k.startswith("mesh.")})
+    vfields = {k[9:]: v for k, v in arr.items() if k.startswith("vertical.")}
+    for k in ("cf1", "cf2", "cf3"):
+        vfields[k] = float(vfields[k])
+    vfields["first_height_level"] = int(vfields["first_height_level"])
+    vertical = VerticalGridData(**vfields)
+    ns = SimpleNamespace(mesh=mesh, vertical=vertical)
+    for k in ("zb_cell", "zb3_cell", "rho_base", "rho_theta_base", "pressure_base", "exner_base",
+              "rho", "rho_theta", "rho_u", "rho_w", "scalars", "adv_coefs", "adv_coefs_3rd",
+              "n_adv_cells_for_edge", "adv_cells_for_edge", "u_init", "v_init"):
+        setattr(ns, k, arr[k])
+    ns.time_seconds = 0.0
+    return ns
+
+
+def differing_words(a, b) -> int:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    assert a.shape == b.shape, (a.shape, b.shape)
+    return int(np.count_nonzero(a.view(np.uint32) != b.view(np.uint32)))

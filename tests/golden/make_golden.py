@@ -1,0 +1,118 @@
+"""Generate the golden step fixtures by running the reference itself.
+
+Runs the reference's CPU dycore authority (``hexcore.driver.DryDycoreDriver``
+with ``V841DryDycoreConfig``, gpuwm-hex 0.5.0) on small synthetic cases built
+by ``hexdyn.case`` and stores inputs and outputs as ``.npz`` fixtures.  It
+needs the reference checkout (default ``/root/reference``) and therefore runs
+only where that exists; the fixtures it writes are what the tests read.
+
+Harness: a two-class ``netCDF4`` stub and a ``gpuwm``
+stub are put on ``sys.path`` (the reference imports them only for file I/O
+and LES route checks); the advection coefficients, vertical grid and terrain
+metrics the reference would take from its Rust engines are supplied by the
+case builder.  The ``native`` fixture wraps the driver so that
+``_advance_dynamics_subcycle`` receives the moist coefficients of every
+carried scalar (``hexcore/regional_v841.py:1180``), which is what native MPAS
+and the reference's CUDA driver apply with physics off.
+
+Usage: python tests/golden/make_golden.py [/path/to/reference]
+"""
+
+from __future__ import annotations
+
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT / "gpuwm-hex_b200"))
+
+from hexdyn.case import build_case, case_arrays  # noqa: E402
+from hexdyn.mesh import build_mesh  # noqa: E402
+
+CASES = {
+    # name: (mesh level, levels, condensates, dt, sub steps, steps, native moist)
+    "l2_L12": (2, 12, 1, 1800.0, 2, 2, True),
+    "l3_L20": (3, 20, 0, 1800.0, 2, 1, False),
+}
+
+
+def _stubs() -> str:
+    d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
+    (d / "netCDF4").mkdir()
+    (d / "netCDF4" / "__init__.py").write_text(
+        "class Dataset:\n    def __init__(self, *a, **k):\n        raise RuntimeError('no netCDF I/O')\n"
+        "class Variable:\n    pass\n")
+    (d / "gpuwm").mkdir()
+    (d / "gpuwm" / "__init__.py").write_text("")
+    (d / "gpuwm" / "backend.py").write_text(
+        "def compilation_target(*a, **k):\n    raise RuntimeError('no gpuwm')\n")
+    return str(d)
+
+
+def main(reference_root: str = "/root/reference") -> None:
+    sys.path.insert(0, _stubs())
+    sys.path.insert(0, str(Path(reference_root) / "tree" / "src"))
+    from hexcore.config_v841 import V841DryDycoreConfig
+    from hexcore.driver import DryDycoreDriver, DryReferenceState, TerrainMetrics
+    from hexcore.dynamics_v841 import V841ReferenceWindProfiles
+    from hexcore.regional_v841 import compute_moist_coefficients
+    from hexcore.state import PrognosticState
+    from hexcore.transport import AdvectionCoefficients
+    from hexcore.vertical import VerticalGrid
+
+    class NativeMoistDriver(DryDycoreDriver):
+        """Moist coefficients of every carried scalar in each subcycle.  With
+        split transport the subcycle's scalars are the step's, so this equals
+        forming them once per step as native MPAS does."""
+
+        def _advance_dynamics_subcycle(self, state, **kw):
+            qtot, cqw, cqu = compute_moist_coefficients(
+                state.scalars, moist_indices=range(state.scalars.shape[0]),
+                cells_on_edge_remapped=np.asarray(self.mesh.cellsOnEdge), nlev=self.nlev)
+            kw.update(moist_cqu=cqu, moist_cqw=cqw, moist_qtot=qtot)
+            return super()._advance_dynamics_subcycle(state, **kw)
+
+    for name, (level, nlev, ncond, dt, nsub, nsteps, native) in CASES.items():
+        t0 = time.time()
+        mesh = build_mesh(level, lloyd=20, seed=0)
+        case = build_case(mesh, n_levels=nlev, seed=0, n_condensates=ncond)
+        vg = VerticalGrid(**{k: getattr(case.vertical, k) for k in case.vertical.__dataclass_fields__})
+        ref = DryReferenceState(case.rho_base, case.rho_theta_base, case.pressure_base, case.exner_base)
+        tm = TerrainMetrics(case.zb_cell, case.zb3_cell)
+        ac = AdvectionCoefficients(case.adv_coefs, case.adv_coefs_3rd, case.n_adv_cells_for_edge,
+                                   case.adv_cells_for_edge, 3, None)
+        wp = V841ReferenceWindProfiles(case.u_init, case.v_init)
+        cfg = V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, config_dynamics_split_steps=3,
+                                  config_split_dynamics_transport=True, config_monotonic=True,
+                                  config_positive_definite=False, config_coef_3rd_order=0.25,
+                                  config_apvm_upwinding=0.5)
+        out = {f"in.{k}": v for k, v in case_arrays(case).items()}
+        out["config.dt"] = dt
+        out["config.n_sub_steps"] = nsub
+        runs = [("dry", DryDycoreDriver)] + ([("native", NativeMoistDriver)] if native else [])
+        for label, cls in runs:
+            drv = cls(mesh, vg, ref, cfg, advection_coefficients=ac, terrain_metrics=tm,
+                      reference_wind_profiles=wp)
+            state = PrognosticState(case.rho.copy(), case.rho_theta.copy(), case.rho_u.copy(),
+                                    case.rho_w.copy(), case.scalars.copy(), 0.0)
+            side = None
+            for step in range(1, (nsteps if label == "dry" else 1) + 1):
+                res = drv.step(state, saved_diagnostics=side)
+                state, side = res.state, res.saved_diagnostics
+                for k in ("rho", "rho_theta", "rho_u", "rho_w", "scalars"):
+                    out[f"{label}.step{step}.{k}"] = np.asarray(getattr(state, k))
+                for k in ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
+                          "pressure_perturbation", "normal_velocity", "vertical_velocity"):
+                    out[f"{label}.step{step}.side.{k}"] = np.asarray(getattr(side, k))
+        path = HERE / f"step_{name}.npz"
+        np.savez_compressed(path, **out)
+        print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -1,0 +1,44 @@
+"""Configuration refusals (hexcore/config_v841.py and hexcore/driver.py:232)."""
+
+import pytest
+
+from hexdyn.config import ConfigurationRefusal, DycoreConfig
+from oracle.dycore import schedule
+
+
+def test_defaults_validate():
+    DycoreConfig().validate()
+
+
+@pytest.mark.parametrize("kw,knob", [
+    (dict(config_dt=-1.0), "config_dt"),
+    (dict(config_time_integration_order=2), "config_time_integration_order"),
+    (dict(config_dynamics_split_steps=2), "config_dynamics_split_steps"),
+    (dict(config_split_dynamics_transport=False), "config_split_dynamics_transport"),
+    (dict(config_smdiv=0.0), "config_smdiv"),
+    (dict(config_divergence_damping=False), "config_divergence_damping"),
+    (dict(config_xnutr=0.2), "config_xnutr"),
+    (dict(config_horiz_mixing="2d_smagorinsky"), "config_horiz_mixing"),
+    (dict(config_moist_physics=True), "config_moist_physics"),
+    (dict(moist_coefficients="wet"), "moist_coefficients"),
+])
+def test_refusals_name_the_knob(kw, knob):
+    with pytest.raises(ConfigurationRefusal) as err:
+        DycoreConfig(**kw).validate()
+    assert err.value.knob == knob
+
+
+def test_unknown_option_refused():
+    with pytest.raises(ConfigurationRefusal):
+        DycoreConfig.from_mapping({"config_les_model": "3d_smagorinsky"})
+
+
+def test_rk3_schedule_matches_mpas():
+    """hexcore/integration.py:104: split 3, 2 sub-steps at dt=1800."""
+    st = schedule(1800.0, 2, 3)
+    assert [s[0] for s in st] == [1, 2, 3]
+    assert [s[1] for s in st] == [200.0, 300.0, 600.0]
+    assert [s[2] for s in st] == [200.0, 300.0, 300.0]
+    assert [s[3] for s in st] == [1, 1, 2]
+    st6 = schedule(720.0, 6, 3)
+    assert [s[3] for s in st6] == [1, 3, 6]

@@ -1,0 +1,124 @@
+"""CUDA step parity through the C ABI.
+
+Strict numerics must reproduce the reference's own outputs word for word
+(golden fixtures made by running the reference, tests/golden/make_golden.py)
+and the oracle at the C1 size (2562 cells x 55 levels).  Fast numerics must
+stay within relative L2 1e-5 per field after one step.
+"""
+
+import numpy as np
+import pytest
+
+import hexdyn
+from fixtures import SIDE, STATE, case_from_arrays, differing_words, inputs, load_golden
+from hexdyn.case import build_case, case_arrays
+from hexdyn.config import DycoreConfig
+from hexdyn.mesh import build_mesh
+from oracle.dycore import OracleConfig, OracleDycore, State
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("these tests need a CUDA GPU")
+    torch.cuda.set_device(0)
+
+
+def make_driver(arr, dt, nsub, moist, numerics="strict", graph=False):
+    case = case_from_arrays(arr)
+    cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, moist_coefficients=moist, numerics=numerics)
+    return hexdyn.from_case(case, cfg, capture_graph=graph)
+
+
+@pytest.mark.parametrize("name,label,steps", [("l2_L12", "dry", 2), ("l2_L12", "native", 1), ("l3_L20", "dry", 1)])
+def test_strict_step_matches_reference_outputs(name, label, steps):
+    fx = load_golden(name)
+    drv = make_driver(inputs(fx), float(fx["config.dt"]), int(fx["config.n_sub_steps"]), label)
+    for step in range(1, steps + 1):
+        res = drv.step()
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), fx[f"{label}.step{step}.{k}"]) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), fx[f"{label}.step{step}.side.{k}"]) == 0, (step, k)
+    drv.close()
+
+
+@pytest.fixture(scope="module")
+def c1_case():
+    mesh = build_mesh(4, lloyd=20, seed=0)
+    return case_arrays(build_case(mesh, n_levels=55, seed=0, n_condensates=0))
+
+
+@pytest.mark.parametrize("moist", ["dry", "native"])
+def test_strict_c1_matches_oracle_two_steps(c1_case, moist):
+    arr = c1_case
+    orc = OracleDycore(arr, OracleConfig(dt=1800.0, n_sub_steps=2, moist=moist))
+    drv = make_driver(arr, 1800.0, 2, moist)
+    st = State(*(np.asarray(arr[k]).copy() for k in STATE))
+    sd = None
+    for step in (1, 2):
+        st, sd = orc.step(st, sd)
+        res = drv.step()
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), getattr(st, k)) == 0, (moist, step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), getattr(sd, k)) == 0, (moist, step, k)
+    drv.close()
+
+
+def test_graph_replay_is_bitwise_eager():
+    fx = load_golden("l2_L12")
+    arr = inputs(fx)
+    eager = make_driver(arr, 1800.0, 2, "native")
+    graph = make_driver(arr, 1800.0, 2, "native", graph=True)
+    for _ in range(3):
+        a, b = eager.step(), graph.step()
+    for k in STATE:
+        assert differing_words(getattr(a.state, k), getattr(b.state, k)) == 0, k
+    assert b.receipt.graph
+    eager.close()
+    graph.close()
+
+
+def test_fast_numerics_within_tolerance(c1_case):
+    strict = make_driver(c1_case, 1800.0, 2, "native")
+    fast = make_driver(c1_case, 1800.0, 2, "native", numerics="fast")
+    a, b = strict.step(), fast.step()
+    for k in STATE:
+        x = getattr(a.state, k).astype(np.float64)
+        y = getattr(b.state, k).astype(np.float64)
+        if k == "rho_w":
+            # rw starts at zero: compare against the field's own scale
+            rel = np.linalg.norm(x - y) / max(np.linalg.norm(x), 1e-30)
+            assert rel < 1e-3, (k, rel)
+            continue
+        rel = np.linalg.norm(x - y) / np.linalg.norm(x)
+        assert rel <= 1e-5, (k, rel)
+    strict.close()
+    fast.close()
+
+
+def test_runs_are_deterministic(c1_case):
+    outs = []
+    for _ in range(2):
+        drv = make_driver(c1_case, 1800.0, 2, "native")
+        outs.append(drv.step())
+        drv.close()
+    for k in STATE:
+        assert differing_words(getattr(outs[0].state, k), getattr(outs[1].state, k)) == 0
+
+
+def test_validation_flag_raises_on_bad_state():
+    """A host-side corruption (negative rho_theta in one column) must come back
+    as the device validation flag, not as a silent result or a fault."""
+    fx = load_golden("l2_L12")
+    arr = dict(inputs(fx))
+    arr["rho_theta"] = arr["rho_theta"].copy()
+    arr["rho_theta"][:, 5] = -arr["rho_theta"][:, 5]
+    with pytest.raises(FloatingPointError):
+        drv = make_driver(arr, 1800.0, 2, "dry")
+        drv.step()

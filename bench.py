@@ -1,0 +1,404 @@
+"""Benchmark: simulated days per wall-hour of the MPAS-A v8.4.2 dry-plus-tracer
+dycore step on the x1.40962 mesh, 55 levels, FP32.
+
+Workload (default): the bisected icosahedron at level 6 (40962 cells, 122880
+edges, 81920 vertices), 55 levels to 30 km, the balanced jet with terrain,
+qv plus 5 condensate tracers, dt = 720 s, 2 acoustic sub-steps, split-3 RK3,
+monotonic FCT, native moist coefficients, strict numerics (bit-identical to
+the reference authority), the whole large step replayed as one CUDA graph.
+Synthetic inputs stand in for the reference's x1.40962 grid/init files.
+
+One JSON line is printed by rank 0.  ``--impl reference`` times the
+reference's CPU step path restated in NumPy (the oracle) on the host cores
+on the same workload instead.
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torch.distributed.run, one process per GPU, each advancing its own replica
+(the single-instance step does not shard: replicas only).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "gpuwm-hex_b200"))
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+LEVEL_DT = {4: 1800.0, 5: 1440.0, 6: 720.0, 7: 360.0}
+METRIC = "simulated days/wall-hour, x1.40962 55L FP32: plain vs batched vs learned-corrected"
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=6)
+    ap.add_argument("--levels", type=int, default=55)
+    ap.add_argument("--condensates", type=int, default=5)
+    ap.add_argument("--numerics", default="strict", choices=["strict", "fast"])
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=60.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------- byte model
+def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 6, advW: int = 10) -> int:
+    """Algorithmic bytes of one launch: each distinct array read or written,
+    times the extent it touches (L levels or L+1 interfaces per entity), 4 B,
+    counted once; connectivity/coefficient tables counted once."""
+    cl, ci, el, vl = C * L, C * (L + 1), E * L, V * L
+    tcl, tel = T * C * L, T * E * L
+    conn_c = C * maxE * 3 + C * 2          # eoc, csign (+ coc/voc) and deg, inv_area
+    conn_e = E * 2 + E * 4                 # coe and per-edge metrics
+    adv = E * advW * 3                     # adv, adv3, adv_cells
+    zb = 2 * C * maxE * (L + 1)
+    words = {
+        "k_diag_vertex": el + 2 * vl + V * 8,
+        "k_diag_cell": el + 2 * vl + 2 * cl + conn_c,
+        "k_diag_edge": 3 * el + vl + cl + conn_e + E * 24,
+        "k_moist_cell": tcl + 2 * cl,
+        "k_moist_edge": tcl + el + conn_e,
+        "k_euler_edge": 3 * el + 4 * cl + conn_e,
+        "k_euler_cell": el + 2 * ci + 5 * cl + conn_c,
+        "k_hdiv": el + cl + conn_c,
+        "k_edge_adv": 3 * el + cl + ci + adv,
+        "k_tend_u": 4 * el + ci + 3 * cl + conn_e + E * 24,
+        "k_tend_cell": 5 * el + 5 * ci + 4 * cl + zb + conn_c,
+        "k_vcoef": 9 * cl + 6 * cl + ci,
+        "k_ac_edge": 7 * el + 6 * cl + conn_e,
+        "k_ac_cell": el + 16 * cl + 9 * ci + conn_c,
+        "k_recover_edge": 7 * el + 3 * cl + conn_e,
+        "k_recover_cell": el + 15 * cl + 7 * ci + zb + conn_c,
+        "k_tr_edge": (tcl + tel) + el + adv,
+        "k_tr_std": 3 * tcl + tel + 2 * cl + el + ci + conn_c,
+        "k_fct_target": 2 * cl + el + ci + conn_c,
+        "k_fct_cell1": 5 * tcl + tel + 2 * cl + el + ci + conn_c,
+        "k_fct_edge": 3 * tcl + 2 * tel + el + conn_e,
+        "k_fct_cell2": 6 * tcl + tel + cl + ci + conn_c,
+    }
+    if name not in words:
+        return 0
+    return 4 * int(words[name])
+
+
+def measured_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) of the SM clock and throttle reasons."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[4]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [r for r in rows if r[2] > 0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median([r[0] for r in loaded])), "sm_max_mhz": max(r[1] for r in loaded),
+                "reasons": reasons, "samples": len(loaded)}
+
+
+# ---------------------------------------------------------------- helpers
+def build_workload(args):
+    from hexdyn.case import build_case
+    from hexdyn.mesh import build_mesh
+
+    mesh = build_mesh(args.level, lloyd=20, seed=0)
+    return build_case(mesh, n_levels=args.levels, seed=0, n_condensates=args.condensates)
+
+
+def workload_config(args, case) -> dict:
+    m = case.mesh
+    return {
+        "workload": f"x1.{m.n_cells} synthetic icosahedral Voronoi mesh (bisection level {args.level}, 20 Lloyd "
+                    f"iterations), {args.levels} levels to 30 km, balanced jet + terrain, "
+                    f"{case.scalars.shape[0]} tracers, dt={LEVEL_DT[args.level]:g} s, 2 acoustic sub-steps, "
+                    "split-3 RK3, monotonic FCT",
+        "cells": m.n_cells, "edges": m.n_edges, "vertices": m.n_vertices, "levels": args.levels,
+        "tracers": int(case.scalars.shape[0]), "dt_s": LEVEL_DT[args.level], "path": "plain",
+        "numerics": args.numerics, "moist_coefficients": "native",
+        "l2": "inputs larger than L2 (per-step working set > 126 MB)",
+        "graph": not args.no_graph,
+    }
+
+
+def oracle_time_per_step(case, dt: float, budget_s: float, max_steps: int) -> tuple[float, int]:
+    from hexdyn.case import case_arrays
+    from oracle.dycore import OracleConfig, OracleDycore, State
+
+    arr = case_arrays(case)
+    orc = OracleDycore(arr, OracleConfig(dt=dt, n_sub_steps=2, moist="native"))
+    st = State(*(np.asarray(arr[k]).copy() for k in ("rho", "rho_theta", "rho_u", "rho_w", "scalars")))
+    sd = None
+    times = []
+    t_all = time.perf_counter()
+    while len(times) < max_steps:
+        t0 = time.perf_counter()
+        st, sd = orc.step(st, sd)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget_s:
+            break
+    return float(np.mean(times)), len(times)
+
+
+def cores_used() -> int:
+    return 1
+
+
+# ------------------------------------------------------------------- arms
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    case = build_workload(args)
+    dt = LEVEL_DT[args.level]
+    budget = max(30.0, min(170.0, args.cpu_budget_s * 2.5))
+    sec, n = oracle_time_per_step(case, dt, budget, max(1, args.steps))
+    value = (dt / 86400.0) / (sec / 3600.0)
+    sample = (f"{n} full large step(s) of the {case.mesh.n_cells}-cell workload (of --steps {args.steps} "
+              f"requested; bounded to ~{budget:.0f} s), no warm-up needed for NumPy")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "simulated days/hour",
+        "n_gpus": 0, "steps": n, "warmup": 0, "ms_per_step": sec * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, case),
+        "cpu_baseline": {"value": value, "unit": "simulated days/hour", "cores": cores_used(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "simulated days/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+
+    import hexdyn
+    from hexdyn.config import DycoreConfig
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+    dt = LEVEL_DT[args.level]
+    case = build_workload(args)
+    cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=2, moist_coefficients="native",
+                       numerics=args.numerics)
+    drv = hexdyn.from_case(case, cfg, capture_graph=not args.no_graph)
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[0])
+                           if world == 1 else local_rank).start()
+    drv.step_async(max(3, args.warmup))
+    drv.read_flag()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    drv.step_async(args.steps)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    elapsed = start.elapsed_time(stop)
+    flag = drv.read_flag()
+    if dist is not None:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    clocks = sampler.stop()
+    ms_per_step = elapsed / args.steps
+    days = args.steps * dt / 86400.0
+    value = world * days / (elapsed / 1000.0 / 3600.0)
+    launches = drv.receipt().launches_per_step
+
+    # per-kernel CUDA-event profile over the same number of eager steps
+    prof = drv.profile(max(1, min(args.steps, 20)))
+    prof_steps = max(1, min(args.steps, 20))
+    C, E, V = case.mesh.n_cells, case.mesh.n_edges, case.mesh.n_vertices
+    L, T = args.levels, int(case.scalars.shape[0])
+    peak, peak_kind = measured_peak()
+    total_ms = sum(ms for _, ms in prof.values())
+    kernels = {}
+    for name, (n, ms) in prof.items():
+        avg_ms = ms / n
+        b = kernel_bytes(name, C, E, V, L, T, advW=int(case.adv_cells_for_edge.shape[1]))
+        kernels[name] = {"launches_per_step": n / prof_steps, "avg_us": avg_ms * 1000.0,
+                         "share": ms / total_ms, "bytes": b,
+                         "gbs": (b / (avg_ms / 1000.0) / 1e9) if b else None}
+    dominant = max(kernels, key=lambda k: kernels[k]["share"])
+    dk = kernels[dominant]
+    achieved = dk["gbs"]
+    traffic = None
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        try:
+            traffic = json.loads(traffic_file.read_text()).get(dominant)
+        except Exception:  # noqa: BLE001
+            traffic = None
+    step_bytes = sum(kernel_bytes(k, C, E, V, L, T) * kernels[k]["launches_per_step"] for k in kernels)
+
+    # end to end through host buffers: upload state+sidecar, step, download
+    from hexdyn import _lib
+
+    def pinned(shape):
+        t = torch.empty(int(np.prod(shape)), dtype=torch.float32, pin_memory=True)
+        return t.numpy().reshape(shape), t
+
+    state_now, side_now = drv.get_state()
+    hold = []
+    sin, sdin, sout, sdout = {}, {}, {}, {}
+    for name in _lib.STATE_FIELDS:
+        a, t = pinned(drv.field_shape(name))
+        a[...] = getattr(state_now, name)
+        sin[name] = a
+        b, t2 = pinned(drv.field_shape(name))
+        sout[name] = b
+        hold += [t, t2]
+    for name in _lib.SIDECAR_FIELDS:
+        a, t = pinned(drv.field_shape(name))
+        a[...] = getattr(side_now, name)
+        sdin[name] = a
+        b, t2 = pinned(drv.field_shape(name))
+        sdout[name] = b
+        hold += [t, t2]
+    h2d = sum(a.nbytes for a in (*sin.values(), *sdin.values()))
+    d2h = sum(a.nbytes for a in (*sout.values(), *sdout.values()))
+    e2e_steps = max(3, min(args.steps, 20))
+    drv.step_host_buffers(sin, sdin, sout, sdout)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        drv.step_host_buffers(sin, sdin, sout, sdout)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * (e2e_steps * dt / 86400.0) / (e2e_ms / 1000.0 / 3600.0)
+    drv.read_flag()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, n = oracle_time_per_step(case, dt, args.cpu_budget_s, 2)
+        cpu = {"value": (dt / 86400.0) / (sec / 3600.0), "unit": "simulated days/hour", "cores": cores_used(),
+               "kind": "port",
+               "sample": f"{n} full large step(s) of this workload by the NumPy oracle (single thread), "
+                         f"{sec:.1f} s/step"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "simulated days/hour", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(args, case),
+            "parallelism": "replicas" if world > 1 else "single instance",
+            "clocks": clocks, "validation_flag": flag,
+            "e2e": {"value": e2e_value, "unit": "simulated days/hour", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": int(launches) * args.steps if not args.no_graph else int(launches) * args.steps,
+            "gpu_launches_per_step": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "traffic": traffic, "bytes_per_launch": dk["bytes"], "avg_launch_us": dk["avg_us"],
+                         "share": dk["share"]},
+            "step_bytes_algorithmic": step_bytes,
+            "step_gbs": step_bytes / (ms_per_step / 1000.0) / 1e9,
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    drv.close()
+    del hold
+
+
+def main() -> None:
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            run_ours(args, rank, world, local_rank)
+        finally:
+            dist.destroy_process_group()
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

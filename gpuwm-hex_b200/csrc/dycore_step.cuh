@@ -5,27 +5,39 @@
 struct Launcher {
   HexCtx& ctx;
   cudaStream_t st;
+  std::vector<HexProfEvent>* prof = nullptr;  // per-launch CUDA events when profiling
   long long count = 0;
   cudaError_t err = cudaSuccess;
   int epb() const { return ctx.geo.S >= 256 ? 1 : 256 / ctx.geo.S; }
   template <class K, class... A>
-  void lp(int n, int nz, size_t smem_per_entity, K kernel, A... args) {
+  void lp(const char* name, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
     if (err != cudaSuccess || n <= 0 || nz <= 0) return;
     const int e = epb();
     dim3 block(ctx.geo.S, e), grid((n + e - 1) / e, 1, nz);
+    HexProfEvent ev{name, nullptr, nullptr};
+    if (prof) {
+      cudaEventCreate(&ev.start);
+      cudaEventCreate(&ev.stop);
+      cudaEventRecord(ev.start, st);
+    }
     kernel<<<grid, block, smem_per_entity * e, st>>>(args...);
     ++count;
     err = cudaGetLastError();
+    if (prof) {
+      cudaEventRecord(ev.stop, st);
+      prof->push_back(ev);
+    }
   }
 };
+#define LP(L, n, nz, smem, kernel, ...) (L).lp(#kernel, n, nz, smem, kernel, __VA_ARGS__)
 
 static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexCtx& c = L.ctx;
   const HexGeo& g = c.geo;
   HexWork& w = c.w;
-  L.lp(g.nV, 1, 0, k_diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
-  L.lp(g.nC, 1, 0, k_diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
-  L.lp(g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex, (const float*)w.pv_cell, w.v, w.pv_edge,
+  LP(L, g.nV, 1, 0, k_diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
+  LP(L, g.nC, 1, 0, k_diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
+  LP(L, g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex, (const float*)w.pv_cell, w.v, w.pv_edge,
        recompute_v);
 }
 
@@ -39,23 +51,24 @@ cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side
 cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream) {
   Launcher L{ctx, stream};
   const HexGeo& g = ctx.geo;
-  L.lp(g.nE, 1, 0, k_recover_u, g, (const float*)s.rho, (const float*)s.rho_u, side.u);
-  L.lp(g.nC, 1, 0, k_rebuild_cell, g, (const float*)s.rho, (const float*)s.rho_theta, (const float*)s.rho_u,
+  LP(L, g.nE, 1, 0, k_recover_u, g, (const float*)s.rho, (const float*)s.rho_u, side.u);
+  LP(L, g.nC, 1, 0, k_rebuild_cell, g, (const float*)s.rho, (const float*)s.rho_theta, (const float*)s.rho_u,
        (const float*)s.rho_w, side, ctx.w.flag);
   return L.err;
 }
 
 cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
-                     const HexSide& side_out, cudaStream_t stream, long long* launches) {
-  Launcher L{ctx, stream};
+                     const HexSide& side_out, cudaStream_t stream, long long* launches,
+                     std::vector<HexProfEvent>* prof) {
+  Launcher L{ctx, stream, prof};
   const HexGeo& g = ctx.geo;
   HexWork& w = ctx.w;
   const int nT = ctx.n_scalars;
   const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * 5;
 
   if (g.moist) {
-    L.lp(g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
-    L.lp(g.nE, 1, 0, k_moist_edge, g, (const float*)in.scalars, nT, w.cqu);
+    LP(L, g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
+    LP(L, g.nE, 1, 0, k_moist_edge, g, (const float*)in.scalars, nT, w.cqu);
   }
   // initial solve diagnostics with v reconstructed (rk_step=3)
   diagnostics(L, side_in.u, 1);
@@ -71,13 +84,13 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
     const int flux_mode = 4 | (sub == 0 ? 1 : 0) | (last ? 2 : 0);
     // vertical coefficients before RK (stage-1 acoustic dts, saved theta)
     {
-      L.lp(g.nC, 1, sm_vcoef, k_vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
+      LP(L, g.nC, 1, sm_vcoef, k_vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
            (const float*)s_in->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
            w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
     }
-    L.lp(g.nE, 1, 0, k_euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
+    LP(L, g.nE, 1, 0, k_euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
          (const float*)w.qtot, (const float*)w.cqu, w.euler_ru);
-    L.lp(g.nC, 1, 0, k_euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
+    LP(L, g.nC, 1, 0, k_euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
          (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
          w.tend_rho, w.euler_rw);
 
@@ -87,16 +100,16 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const HexStage& stg = ctx.dyn[si];
       const float dts = (float)stg.acoustic_dt;
       if (stg.stage == 2) {
-        L.lp(g.nC, 1, sm_vcoef, k_vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
+        LP(L, g.nC, 1, sm_vcoef, k_vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
       }
-      L.lp(g.nC, 1, 0, k_hdiv, g, (const float*)cur->rho_u, w.hdiv);
-      L.lp(g.nE, 1, 0, k_edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
+      LP(L, g.nC, 1, 0, k_hdiv, g, (const float*)cur->rho_u, w.hdiv);
+      LP(L, g.nE, 1, 0, k_edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
            w.edge_theta, w.edge_w);
-      L.lp(g.nE, 1, 0, k_tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
+      LP(L, g.nE, 1, 0, k_tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
            (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
-      L.lp(g.nC, 1, 0, k_tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
+      LP(L, g.nC, 1, 0, k_tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
            (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
            (const float*)w.euler_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage);
@@ -107,18 +120,18 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         const float* old_rt = w.rtpp[(n - 1) & 1];
         float* new_rt = w.rtpp[n & 1];
         if (n == 1) {
-          L.lp(g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
+          LP(L, g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
                old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         } else {
           // damping of substep n-1 (new = its output, old = its input), then update n
           const float* prev_new = w.rtpp[(n - 1) & 1];
           const float* prev_old = w.rtpp[(n - 2) & 1];
-          L.lp(g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
+          LP(L, g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
                prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         }
-        L.lp(g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
+        LP(L, g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
              (const float*)s_in->theta_m, (const float*)w.tend_rho, (const float*)w.tend_rt,
              (const float*)w.tend_rw, (const float*)w.cofwr, (const float*)w.cofwz, (const float*)w.coftz,
              (const float*)w.cofwt, (const float*)w.a_tri, (const float*)w.alpha_tri, (const float*)w.gamma_tri,
@@ -127,7 +140,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       }
       {
         const int n = stg.acoustic_steps;
-        L.lp(g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
+        LP(L, g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
              (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
              (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
       }
@@ -135,10 +148,10 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const float inv_steps = 1.0f / (float)stg.acoustic_steps;
       const float inv_splits = 1.0f / (float)ctx.split_steps;
       const int fm = stg.stage == 3 ? flux_mode : 0;
-      L.lp(g.nE, 1, 0, k_recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
+      LP(L, g.nE, 1, 0, k_recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
            (const float*)w.ru_avg, (const float*)s_in->rho_p, (const float*)w.rho_pp, o.rho_u, so.u, w.flux_u,
            fm, inv_steps, inv_splits);
-      L.lp(g.nC, 1, 0, k_recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
+      LP(L, g.nC, 1, 0, k_recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
            (const float*)s_in->rtheta_p, (const float*)saved->rho_w, (const float*)w.rho_pp, rtpp_final,
            (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
            inv_splits, w.flag);
@@ -159,19 +172,19 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
       if (si < 2 || !ctx.monotonic) {
         const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
-        L.lp(g.nE, nT, 0, k_tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
-        L.lp(g.nC, nT, 0, k_tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LP(L, g.nE, nT, 0, k_tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
+        LP(L, g.nC, nT, 0, k_tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)out.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, q_next);
       } else {
-        L.lp(g.nC, 1, 0, k_fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
+        LP(L, g.nC, 1, 0, k_fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
              (const float*)w.flux_w, w.target, w.flag);
-        L.lp(g.nE, nT, 0, k_tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
-        L.lp(g.nC, nT, 0, k_fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LP(L, g.nE, nT, 0, k_tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
+        LP(L, g.nC, nT, 0, k_fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass);
-        L.lp(g.nE, nT, 0, k_fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
+        LP(L, g.nE, nT, 0, k_fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
-        L.lp(g.nC, nT, 0, k_fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
+        LP(L, g.nC, nT, 0, k_fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
              (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
              (const float*)w.target, q_next);
       }

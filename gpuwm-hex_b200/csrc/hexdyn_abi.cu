@@ -452,17 +452,17 @@ int build(HexDynHandle* h, const HexDynDesc& d) {
 HexState cur_state(HexDynHandle* h) { return h->ctx.parity ? h->ctx.out : h->ctx.in; }
 HexSide cur_side(HexDynHandle* h) { return h->ctx.parity ? h->ctx.side_out : h->ctx.side_in; }
 
-cudaError_t enqueue_step(HexDynHandle* h, cudaStream_t st) {
+cudaError_t enqueue_step(HexDynHandle* h, cudaStream_t st, std::vector<HexProfEvent>* prof = nullptr) {
   HexCtx& c = h->ctx;
   const int p = c.parity;
-  if (c.graph_exec[p]) return cudaGraphLaunch(c.graph_exec[p], st);
+  if (c.graph_exec[p] && !prof) return cudaGraphLaunch(c.graph_exec[p], st);
   const HexState& in = p ? c.out : c.in;
   const HexState& out = p ? c.in : c.out;
   const HexSide& si = p ? c.side_out : c.side_in;
   const HexSide& so = p ? c.side_in : c.side_out;
   long long launches = 0;
-  cudaError_t e = c.numerics ? hexdyn_fast::run_step(c, in, si, out, so, st, &launches)
-                             : hexdyn_strict::run_step(c, in, si, out, so, st, &launches);
+  cudaError_t e = c.numerics ? hexdyn_fast::run_step(c, in, si, out, so, st, &launches, prof)
+                             : hexdyn_strict::run_step(c, in, si, out, so, st, &launches, prof);
   c.launches_per_step = launches;
   return e;
 }
@@ -555,6 +555,49 @@ int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps) {
     h->ctx.steps_done++;
   }
   return HEXDYN_OK;
+}
+
+int hexdyn_profile_steps(HexDynHandle* h, void* stream, int nsteps, char* out, size_t len) {
+  if (!h || !out || len == 0) return fail(HEXDYN_E_ARG, "NULL argument");
+  if (nsteps <= 0) return fail(HEXDYN_E_ARG, "nsteps must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<HexProfEvent> prof;
+  prof.reserve(4096);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
+    e = enqueue_step(h, st, &prof);
+    h->ctx.parity ^= 1;
+    h->ctx.steps_done++;
+  }
+  cudaError_t se = cudaStreamSynchronize(st);
+  std::vector<std::string> names;
+  std::vector<double> total;
+  std::vector<long long> count;
+  for (auto& ev : prof) {
+    float ms = 0.0f;
+    if (e == cudaSuccess && se == cudaSuccess) cudaEventElapsedTime(&ms, ev.start, ev.stop);
+    size_t i = 0;
+    while (i < names.size() && names[i] != ev.name) ++i;
+    if (i == names.size()) {
+      names.push_back(ev.name);
+      total.push_back(0.0);
+      count.push_back(0);
+    }
+    total[i] += ms;
+    count[i] += 1;
+    cudaEventDestroy(ev.start);
+    cudaEventDestroy(ev.stop);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "profile step");
+  if (se != cudaSuccess) return cuda_fail(se, "profile sync");
+  std::string text;
+  char line[256];
+  for (size_t i = 0; i < names.size(); ++i) {
+    snprintf(line, sizeof line, "%s %lld %.6f\n", names[i].c_str(), count[i], total[i]);
+    text += line;
+  }
+  snprintf(out, len, "%s", text.c_str());
+  return text.size() < len ? HEXDYN_OK : fail(HEXDYN_E_CAPACITY, "profile text needs %zu bytes", text.size() + 1);
 }
 
 int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out) {

@@ -45,6 +45,11 @@ struct HexWork {
   int* flag;            // device validation flag (bit set, see HEX_FLAG_*)
 };
 
+struct HexProfEvent {   // one profiled launch: kernel name and its bracketing events
+  const char* name;
+  cudaEvent_t start, stop;
+};
+
 struct HexStage {
   int stage;            // 1..3
   double large_dt;
@@ -77,13 +82,15 @@ struct HexCtx {
 
 namespace hexdyn_strict {
 cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
-                     const HexSide& side_out, cudaStream_t stream, long long* launches);
+                     const HexSide& side_out, cudaStream_t stream, long long* launches,
+                     std::vector<HexProfEvent>* prof);
 cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
 cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
 }  // namespace hexdyn_strict
 namespace hexdyn_fast {
 cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, const HexState& out,
-                     const HexSide& side_out, cudaStream_t stream, long long* launches);
+                     const HexSide& side_out, cudaStream_t stream, long long* launches,
+                     std::vector<HexProfEvent>* prof);
 cudaError_t rebuild_sidecar(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
 cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream);
 }  // namespace hexdyn_fast

@@ -66,6 +66,7 @@ EXPORTS = {
     "hexdyn_step_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "hexdyn_read_flag": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "hexdyn_capture_graph": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hexdyn_profile_steps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
     "hexdyn_device_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "hexdyn_level_stride": (C.c_int, [C.c_void_p]),
     "hexdyn_launches_per_step": (C.c_longlong, [C.c_void_p]),

@@ -326,19 +326,29 @@ def terrain_metrics(mesh: VoronoiMesh, vertical: VerticalGridData, d2: np.ndarra
 # ------------------------------------------------------------- atmosphere
 
 
+def jet_profile(z: np.ndarray, z_jet: float = 10000.0, decay: float = 8000.0) -> tuple[np.ndarray, np.ndarray]:
+    """Vertical shape of the jet and its derivative: linear from 0 at the
+    ground to 1 at ``z_jet``, Gaussian decay above."""
+    z = np.asarray(z, dtype=np.float64)
+    below = z <= z_jet
+    vz = np.where(below, z / z_jet, np.exp(-((z - z_jet) / decay) ** 2))
+    dvz = np.where(below, 1.0 / z_jet, -2.0 * (z - z_jet) / decay ** 2 * np.exp(-((z - z_jet) / decay) ** 2))
+    return vz, dvz
+
+
 def _balanced_jet(u0: float, z_jet: float, theta0: float, n2: float,
                   radius: float, n_lat: int = 1441, dz: float = 50.0, ztop: float = 34000.0):
     """theta(lat, z) and exner(lat, z) in hydrostatic + gradient-wind balance.
 
-    u = u0 sin^2(2 lat) (z/z_jet) exp(1 - z/z_jet) vanishes at the ground, so
-    the surface Exner function is uniform (1) and the balance reduces to the
-    thermal-wind equation g dlnθ/dlat + F dlnθ/dz = dF/dz with
-    F = a f u + u^2 tan(lat), marched from the equator with RK2.
+    u = u0 sin^2(2 lat) V(z) with V(0) = 0, so the surface Exner function is
+    uniform (1).  Cross-differentiating the gradient-wind balance
+    dπ/dlat = -F/(cp θ), F = a f u + u^2 tan(lat), with the hydrostatic
+    dπ/dz = -g/(cp θ) gives the thermal-wind equation
+    g dlnθ/dlat = F dlnθ/dz - dF/dz, marched from the equator with RK2.
     """
     z = np.arange(0.0, ztop + dz, dz)
     lat = np.linspace(-np.pi / 2, np.pi / 2, n_lat)
-    vz = (z / z_jet) * np.exp(1.0 - z / z_jet)
-    dvz = (1.0 / z_jet - z / z_jet ** 2) * np.exp(1.0 - z / z_jet)
+    vz, dvz = jet_profile(z, z_jet)
 
     def forcing(phi: float) -> tuple[np.ndarray, np.ndarray]:
         s, c = np.sin(phi), np.cos(phi)
@@ -352,7 +362,7 @@ def _balanced_jet(u0: float, z_jet: float, theta0: float, n2: float,
     def rhs(phi: float, ln_theta: np.ndarray) -> np.ndarray:
         big_f, big_fz = forcing(phi)
         lz = np.gradient(ln_theta, dz)
-        return (big_fz - big_f * lz) / GRAVITY
+        return (big_f * lz - big_fz) / GRAVITY
 
     eq = n_lat // 2
     ln_t = np.zeros((n_lat, z.size))
@@ -437,7 +447,7 @@ def build_case(mesh: VoronoiMesh, *, n_levels: int = 55, ztop: float = 30000.0,
     c1, c2 = mesh.cellsOnEdge[:, 0], mesh.cellsOnEdge[:, 1]
     z_edge = 0.5 * (z_mid[:, c1] + z_mid[:, c2])
     lat_e, lon_e = mesh.latEdge, mesh.lonEdge
-    vz = (z_edge / 10000.0) * np.exp(1.0 - z_edge / 10000.0)
+    vz, _ = jet_profile(z_edge)
     u_east = jet_speed * np.sin(2.0 * lat_e)[None, :] ** 2 * vz
     lat0, lon0 = np.deg2rad(40.0), np.deg2rad(20.0)
     cosd = np.sin(lat_e) * np.sin(lat0) + np.cos(lat_e) * np.cos(lat0) * np.cos(lon_e - lon0)

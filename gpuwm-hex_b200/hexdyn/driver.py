@@ -259,6 +259,18 @@ class HexDycoreDriver:
         self.time_seconds += nsteps * self.config.config_dt
         return DeviceStepResult(DeviceAtmosphere(self), self.receipt(nsteps, flag.value))
 
+    def profile(self, nsteps: int = 1) -> dict[str, tuple[int, float]]:
+        """Per-kernel launches and total milliseconds over ``nsteps`` eager
+        steps, each launch bracketed by CUDA events on the driver's stream."""
+        buf = C.create_string_buffer(1 << 16)
+        _lib.check(self._lib.hexdyn_profile_steps(self._handle, self._stream_handle(), int(nsteps), buf, len(buf)))
+        self.time_seconds += nsteps * self.config.config_dt
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, launches, ms = line.split()
+            out[name] = (int(launches), float(ms))
+        return out
+
     def receipt(self, steps: int = 0, flag: int = 0) -> StepReceipt:
         return StepReceipt(steps=steps, flag=flag,
                            launches_per_step=int(self._lib.hexdyn_launches_per_step(self._handle)),
@@ -278,6 +290,25 @@ class HexDycoreDriver:
         state = HostState(**{k: out[k] for k in _lib.STATE_FIELDS}, time_seconds=self.time_seconds)
         side = HostSidecar(**{k: out[k] for k in _lib.SIDECAR_FIELDS})
         return state, side
+
+    def step_host_buffers(self, state_in: dict, side_in: dict, state_out: dict, side_out: dict) -> None:
+        """One large step from host buffers to host buffers, enqueued on the
+        driver's stream without synchronising: upload of the state and sidecar,
+        the step, download of both (the reference's from_host upload, step_device
+        and step() download, hexcore/cuda_driver.py:2826,5751,6112).  Use pinned
+        arrays for asynchronous copies; synchronise before reading the outputs."""
+        st = self._stream_handle()
+        for name, arr in (*state_in.items(), *side_in.items()):
+            _lib.check(self._lib.hexdyn_set_state(self._handle, _lib.FIELDS[name],
+                                                  arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, st))
+        _lib.check(self._lib.hexdyn_step_async(self._handle, st, 1))
+        self.time_seconds += self.config.config_dt
+        for name, arr in (*state_out.items(), *side_out.items()):
+            _lib.check(self._lib.hexdyn_get_state(self._handle, _lib.FIELDS[name],
+                                                  arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, st))
+
+    def field_shape(self, name: str) -> tuple[int, ...]:
+        return self._shape(name)
 
     def step(self, nsteps: int = 1) -> HostStepResult:
         res = self.step_device(nsteps)

@@ -152,6 +152,12 @@ int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps);
 /* Read and clear the validation flag (synchronises `stream`). */
 int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out);
 
+/* Run nsteps eager steps with a CUDA event pair around every kernel launch
+ * and write one line per kernel, "name launches total_ms", into out.
+ * (Profiling entry point; the reference's launch_timed,
+ * hexcore/cuda_subcycle_graphs.py:45-62.) */
+int hexdyn_profile_steps(HexDynHandle* h, void* stream, int nsteps, char* out, size_t len);
+
 /* Capture the whole large step into CUDA graphs (one per buffer parity);
  * later hexdyn_step calls replay them. */
 int hexdyn_capture_graph(HexDynHandle* h, void* stream);

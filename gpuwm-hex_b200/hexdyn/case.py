@@ -326,25 +326,55 @@ def terrain_metrics(mesh: VoronoiMesh, vertical: VerticalGridData, d2: np.ndarra
 # ------------------------------------------------------------- atmosphere
 
 
-def jet_profile(z: np.ndarray, z_jet: float = 10000.0, decay: float = 8000.0) -> tuple[np.ndarray, np.ndarray]:
-    """Vertical shape of the jet and its derivative: linear from 0 at the
-    ground to 1 at ``z_jet``, Gaussian decay above."""
+def jet_profile(z: np.ndarray, z_jet: float = 10000.0, decay: float = 12000.0) -> tuple[np.ndarray, np.ndarray]:
+    """Vertical shape of the jet and its derivative, continuous to first
+    order: sin(pi z / (2 z_jet)) from 0 at the ground to 1 at ``z_jet``, then
+    a Gaussian decay above.  The shear is largest at the ground and decreases
+    upward, so the thermal-wind temperature field stays statically stable."""
     z = np.asarray(z, dtype=np.float64)
     below = z <= z_jet
-    vz = np.where(below, z / z_jet, np.exp(-((z - z_jet) / decay) ** 2))
-    dvz = np.where(below, 1.0 / z_jet, -2.0 * (z - z_jet) / decay ** 2 * np.exp(-((z - z_jet) / decay) ** 2))
+    g = np.exp(-((z - z_jet) / decay) ** 2)
+    arg = 0.5 * np.pi * np.minimum(z, z_jet) / z_jet
+    vz = np.where(below, np.sin(arg), g)
+    dvz = np.where(below, 0.5 * np.pi / z_jet * np.cos(arg), -2.0 * (z - z_jet) / decay ** 2 * g)
     return vz, dvz
 
 
-def _balanced_jet(u0: float, z_jet: float, theta0: float, n2: float,
-                  radius: float, n_lat: int = 1441, dz: float = 50.0, ztop: float = 34000.0):
+def reference_stability(z: np.ndarray, n2_trop: float = 1.0e-4, n2_strat: float = 4.0e-4,
+                        z_trop: float = 12000.0, width: float = 1500.0) -> np.ndarray:
+    """Brunt-Vaisala frequency squared of the equatorial column: tropospheric
+    below ``z_trop``, stratospheric above, joined by a tanh."""
+    return n2_trop + (n2_strat - n2_trop) * 0.5 * (1.0 + np.tanh((np.asarray(z) - z_trop) / width))
+
+
+def equatorial_theta(z: np.ndarray, theta0: float = 300.0) -> np.ndarray:
+    """theta(z) of the equatorial (and base-state) column from its N^2(z)."""
+    z = np.asarray(z, dtype=np.float64)
+    fine = np.arange(0.0, float(np.max(z)) + 100.0, 10.0)
+    n2 = reference_stability(fine)
+    ln = np.log(theta0) + np.concatenate([[0.0], np.cumsum(0.5 * (n2[1:] + n2[:-1]) * 10.0)]) / GRAVITY
+    return np.exp(np.interp(z, fine, ln))
+
+
+def hydrostatic_exner(z: np.ndarray, theta: np.ndarray) -> np.ndarray:
+    """Exner function of a column theta(z), 1 at z[0] = 0 (trapezoidal rule)."""
+    integrand = GRAVITY / (CP * np.asarray(theta))
+    steps = 0.5 * (integrand[..., 1:] + integrand[..., :-1]) * np.diff(z)
+    zeros = np.zeros(integrand.shape[:-1] + (1,))
+    return 1.0 - np.concatenate([zeros, np.cumsum(steps, axis=-1)], axis=-1)
+
+
+def _balanced_jet(u0: float, z_jet: float, theta0: float, radius: float,
+                  n_lat: int = 1441, dz: float = 50.0, ztop: float = 34000.0):
     """theta(lat, z) and exner(lat, z) in hydrostatic + gradient-wind balance.
 
     u = u0 sin^2(2 lat) V(z) with V(0) = 0, so the surface Exner function is
     uniform (1).  Cross-differentiating the gradient-wind balance
     dπ/dlat = -F/(cp θ), F = a f u + u^2 tan(lat), with the hydrostatic
     dπ/dz = -g/(cp θ) gives the thermal-wind equation
-    g dlnθ/dlat = F dlnθ/dz - dF/dz, marched from the equator with RK2.
+    g dlnθ/dlat = F dlnθ/dz - dF/dz, marched from the equator (where θ is the
+    stratified column of ``equatorial_theta``) with RK2.  The result is
+    checked to be statically stable everywhere.
     """
     z = np.arange(0.0, ztop + dz, dz)
     lat = np.linspace(-np.pi / 2, np.pi / 2, n_lat)
@@ -366,7 +396,7 @@ def _balanced_jet(u0: float, z_jet: float, theta0: float, n2: float,
 
     eq = n_lat // 2
     ln_t = np.zeros((n_lat, z.size))
-    ln_t[eq] = np.log(theta0) + n2 * z / GRAVITY
+    ln_t[eq] = np.log(equatorial_theta(z, theta0))
     for direction in (1, -1):
         cur = ln_t[eq].copy()
         j = eq
@@ -378,10 +408,10 @@ def _balanced_jet(u0: float, z_jet: float, theta0: float, n2: float,
             j += direction
             ln_t[j] = cur
     theta = np.exp(ln_t)
-    # Hydrostatic Exner from a uniform surface value of 1 (p_s = 1000 hPa).
-    integrand = GRAVITY / (CP * theta)
-    exner = 1.0 - np.concatenate(
-        [np.zeros((n_lat, 1)), np.cumsum(0.5 * (integrand[:, 1:] + integrand[:, :-1]) * dz, axis=1)], axis=1)
+    exner = hydrostatic_exner(z, theta)
+    n2 = GRAVITY * np.gradient(ln_t, z, axis=1)
+    if n2.min() <= 0.0:
+        raise RuntimeError(f"balanced jet is statically unstable (min N^2 = {n2.min():.3e})")
     return lat, z, theta, exner
 
 
@@ -415,8 +445,8 @@ def build_case(mesh: VoronoiMesh, *, n_levels: int = 55, ztop: float = 30000.0,
     zb_cell, zb3_cell = terrain_metrics(mesh, vertical, d2, coef_3rd_order)
     adv, adv3, n_adv, adv_cells = advection_stencil(mesh, d2)
 
-    theta0, n2 = 300.0, 1.2e-4
-    lat_g, z_g, theta_g, exner_g = _balanced_jet(jet_speed, 10000.0, theta0, n2, radius)
+    theta0 = 300.0
+    lat_g, z_g, theta_g, exner_g = _balanced_jet(jet_speed, 10000.0, theta0, radius)
     zgrid = np.asarray(vertical.zgrid, dtype=np.float64)
     z_mid = 0.5 * (zgrid[:-1] + zgrid[1:])
     lat_c = np.broadcast_to(mesh.latCell[None, :], z_mid.shape)
@@ -432,9 +462,12 @@ def build_case(mesh: VoronoiMesh, *, n_levels: int = 55, ztop: float = 30000.0,
     rho_dry = pressure / (RGAS * theta * exner)
     zz = np.asarray(vertical.zz, dtype=np.float64)
 
-    # Hydrostatic base state: theta_b = theta0 exp(N^2 z/g), analytic Exner.
-    theta_b = theta0 * np.exp(n2 * z_mid / GRAVITY)
-    exner_b = 1.0 - GRAVITY ** 2 / (CP * theta0 * n2) * (1.0 - np.exp(-n2 * z_mid / GRAVITY))
+    # Hydrostatic base state: the equatorial column, interpolated in height.
+    zb_fine = np.arange(0.0, 34000.0 + 10.0, 10.0)
+    thb_fine = equatorial_theta(zb_fine, theta0)
+    exb_fine = hydrostatic_exner(zb_fine, thb_fine)
+    theta_b = np.interp(z_mid, zb_fine, thb_fine)
+    exner_b = np.interp(z_mid, zb_fine, exb_fine)
     pressure_b = P0 * exner_b ** (CP / RGAS)
     rho_b = pressure_b / (RGAS * theta_b * exner_b)
 

@@ -69,7 +69,8 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
     words = {
         "k_diag_vertex": el + 2 * vl + V * 8,
         "k_diag_cell": el + 2 * vl + 2 * cl + conn_c,
-        "k_diag_edge": 3 * el + vl + cl + conn_e + E * 24,
+        "k_diag_edge": 3 * el + vl + cl + conn_e,                  # u, cached v, pv_edge out
+        "k_diag_edge_v": 3 * el + vl + cl + conn_e + E * 24,       # u (+ neighbours), v out, pv_edge out
         "k_moist_cell": tcl + 2 * cl,
         "k_moist_edge": tcl + el + conn_e,
         "k_euler_edge": 3 * el + 4 * cl + conn_e,
@@ -79,7 +80,10 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_tend_u": 4 * el + ci + 3 * cl + conn_e + E * 24,
         "k_tend_cell": 5 * el + 5 * ci + 4 * cl + zb + conn_c,
         "k_vcoef": 9 * cl + 6 * cl + ci,
-        "k_ac_edge": 7 * el + 6 * cl + conn_e,
+        "k_ac_edge_first": 3 * el,                                 # tend_ru in; ru_p, ru_avg out
+        "k_ac_edge": 7 * el + 6 * cl + conn_e,                     # damping of n-1 + update n
+        "k_ac_edge_damp": 2 * el + 3 * cl + conn_e,                # damping only
+        "k_ac_cell_first": el + 12 * cl + 7 * ci + conn_c,        # old perturbations are zero
         "k_ac_cell": el + 16 * cl + 9 * ci + conn_c,
         "k_recover_edge": 7 * el + 3 * cl + conn_e,
         "k_recover_cell": el + 15 * cl + 7 * ci + zb + conn_c,

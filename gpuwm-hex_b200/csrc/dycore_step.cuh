@@ -37,8 +37,8 @@ static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexWork& w = c.w;
   LP(L, g.nV, 1, 0, k_diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
   LP(L, g.nC, 1, 0, k_diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
-  LP(L, g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex, (const float*)w.pv_cell, w.v, w.pv_edge,
-       recompute_v);
+  L.lp(recompute_v ? "k_diag_edge_v" : "k_diag_edge", g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex,
+       (const float*)w.pv_cell, w.v, w.pv_edge, recompute_v);
 }
 
 cudaError_t diagnostics_only(HexCtx& ctx, const HexState& s, const HexSide& side, cudaStream_t stream) {
@@ -120,18 +120,18 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         const float* old_rt = w.rtpp[(n - 1) & 1];
         float* new_rt = w.rtpp[n & 1];
         if (n == 1) {
-          LP(L, g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
+          L.lp("k_ac_edge_first", g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
                old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         } else {
           // damping of substep n-1 (new = its output, old = its input), then update n
           const float* prev_new = w.rtpp[(n - 1) & 1];
           const float* prev_old = w.rtpp[(n - 2) & 1];
-          LP(L, g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
+          L.lp("k_ac_edge", g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
                prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         }
-        LP(L, g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
+        L.lp(n == 1 ? "k_ac_cell_first" : "k_ac_cell", g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
              (const float*)s_in->theta_m, (const float*)w.tend_rho, (const float*)w.tend_rt,
              (const float*)w.tend_rw, (const float*)w.cofwr, (const float*)w.cofwz, (const float*)w.coftz,
              (const float*)w.cofwt, (const float*)w.a_tri, (const float*)w.alpha_tri, (const float*)w.gamma_tri,
@@ -140,7 +140,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       }
       {
         const int n = stg.acoustic_steps;
-        LP(L, g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
+        L.lp("k_ac_edge_damp", g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
              (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
              (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
       }

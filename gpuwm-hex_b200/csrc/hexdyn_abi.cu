@@ -685,3 +685,155 @@ int hexdyn_destroy(HexDynHandle* h) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ no-alloc step
+// hexdyn_step_noalloc: the large step with its scratch in a file-scope device
+// array instead of the handle's workspace (declaration and contract in
+// include/hexdyn.h).
+
+#include <mutex>
+
+#define HEXDYN_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define HEXDYN_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) float g_noalloc_scratch[HEXDYN_NOALLOC_SCRATCH_BYTES / sizeof(float)];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+float* g_noalloc_ptr[HEXDYN_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device with that device current.
+int noalloc_scratch(float** out) {
+  int dev = 0;
+  HEX_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= HEXDYN_NOALLOC_MAX_DEVICES)
+    return fail(HEXDYN_E_CAPACITY, "device %d beyond the %d devices the no-alloc step tracks", dev,
+                HEXDYN_NOALLOC_MAX_DEVICES);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    HEX_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+    g_noalloc_ptr[dev] = (float*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return HEXDYN_OK;
+}
+
+// Bump carver over the scratch array; every buffer starts on 256 bytes.
+struct Carver {
+  float* base;
+  size_t used = 0;  // words
+  float* take(size_t words) {
+    float* p = base ? base + used : nullptr;
+    used += (words + 63) / 64 * 64;
+    return p;
+  }
+};
+
+// Lays out the step's intermediates; with base == nullptr only counts.
+void carve(Carver& cv, const HexCtx& src, HexCtx& c) {
+  const HexGeo& g = src.geo;
+  const size_t CS = (size_t)g.nC * g.S, ES = (size_t)g.nE * g.S, VS = (size_t)g.nV * g.S;
+  const size_t T = std::max(1, src.n_scalars);
+  HexWork& w = c.w;
+  float** cell[] = {&w.qtot, &w.cqw, &w.ke, &w.pv_cell, &w.tend_rho, &w.euler_rw, &w.hdiv, &w.tend_rt,
+                    &w.tend_rw, &w.cofwr, &w.cofwz, &w.coftz, &w.cofwt, &w.a_tri, &w.alpha_tri, &w.gamma_tri,
+                    &w.rw_p, &w.ww_avg, &w.rho_pp, &w.rtpp[0], &w.rtpp[1], &w.flux_w, &w.target};
+  for (float** p : cell) *p = cv.take(CS);
+  float** edge[] = {&w.cqu, &w.v, &w.pv_edge, &w.euler_ru, &w.edge_theta, &w.edge_w, &w.tend_ru, &w.ru_p,
+                    &w.ru_avg, &w.flux_u};
+  for (float** p : edge) *p = cv.take(ES);
+  w.pv_vertex = cv.take(VS);
+  w.ke_vertex = cv.take(VS);
+  float** tcell[] = {&w.q_stage[0], &w.q_stage[1], &w.scale_in, &w.scale_out, &w.mass};
+  for (float** p : tcell) *p = cv.take(T * CS);
+  w.edge_q = cv.take(T * ES);
+  w.hres_lim = cv.take(T * ES);
+  w.flag = (int*)cv.take(1);
+  for (int i = 0; i < 2; ++i) {
+    HexState& t = c.tmp[i];
+    t.rho = cv.take(CS);
+    t.rho_theta = cv.take(CS);
+    t.rho_w = cv.take(CS);
+    t.rho_u = cv.take(ES);
+    t.scalars = nullptr;
+    HexSide& sd = c.side_tmp[i];
+    float** sc[] = {&sd.theta_m, &sd.exner, &sd.rho_p, &sd.rtheta_p, &sd.pressure_p, &sd.w};
+    for (float** p : sc) *p = cv.take(CS);
+    sd.u = cv.take(ES);
+  }
+}
+
+bool fields_of(const HexDynFields* f, int n_scalars, HexState& s, HexSide& side) {
+  for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i)
+    if (!f->field[i] && !(i == HEXDYN_SCALARS && n_scalars == 0)) return false;
+  s = HexState{f->field[HEXDYN_RHO], f->field[HEXDYN_RHO_THETA], f->field[HEXDYN_RHO_U], f->field[HEXDYN_RHO_W],
+               f->field[HEXDYN_SCALARS]};
+  side = HexSide{f->field[HEXDYN_THETA_M], f->field[HEXDYN_EXNER], f->field[HEXDYN_RHO_P],
+                 f->field[HEXDYN_RHO_THETA_P], f->field[HEXDYN_PRESSURE_P], f->field[HEXDYN_U],
+                 f->field[HEXDYN_W]};
+  return true;
+}
+
+}  // namespace
+
+extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, const HexDynFields* out, void* stream,
+                                   int* flag_out) {
+  if (!h || !in || !out) return fail(HEXDYN_E_ARG, "NULL handle or field set");
+  const HexCtx& src = h->ctx;
+  HexState s_in, s_out;
+  HexSide d_in, d_out;
+  if (!fields_of(in, src.n_scalars, s_in, d_in) || !fields_of(out, src.n_scalars, s_out, d_out))
+    return fail(HEXDYN_E_ARG, "every state and sidecar field needs a device pointer");
+  for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i)
+    for (int j = 0; j < HEXDYN_NUM_FIELDS; ++j)
+      if (in->field[i] && in->field[i] == out->field[j])
+        return fail(HEXDYN_E_ARG, "input field %d and output field %d are the same buffer", i, j);
+  // Size check before touching the device.
+  HexCtx c;
+  Carver count{nullptr};
+  carve(count, src, c);
+  const size_t need = count.used * sizeof(float);
+  if (need > HEXDYN_NOALLOC_SCRATCH_BYTES)
+    return fail(HEXDYN_E_CAPACITY, "this mesh needs %zu bytes of step scratch; the no-alloc step holds %u "
+                "(use hexdyn_step)", need, (unsigned)HEXDYN_NOALLOC_SCRATCH_BYTES);
+  float* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  Carver cv{base};
+  carve(cv, src, c);
+  c.numerics = src.numerics;
+  c.n_scalars = src.n_scalars;
+  c.dt = src.dt;
+  c.split_steps = src.split_steps;
+  c.monotonic = src.monotonic;
+  c.geo = src.geo;
+  for (int i = 0; i < 3; ++i) {
+    c.dyn[i] = src.dyn[i];
+    c.scal[i] = src.scal[i];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const HexGeo& g = c.geo;
+  const size_t CS = (size_t)g.nC * g.S, ES = (size_t)g.nE * g.S;
+  // what must start at zero (or one): the flag and the dry coefficients
+  HEX_CUDA(cudaMemsetAsync(c.w.flag, 0, sizeof(int), st), "clear flag");
+  if (!g.moist) {
+    HEX_CUDA(cudaMemsetAsync(c.w.qtot, 0, CS * sizeof(float), st), "clear qtot");
+    k_fill<<<(unsigned)((CS + 255) / 256), 256, 0, st>>>(c.w.cqw, CS, 1.0f);
+    k_fill<<<(unsigned)((ES + 255) / 256), 256, 0, st>>>(c.w.cqu, ES, 1.0f);
+    HEX_CUDA(cudaGetLastError(), "fill dry coefficients");
+  }
+  long long launches = 0;
+  cudaError_t e = c.numerics ? hexdyn_fast::run_step(c, s_in, d_in, s_out, d_out, st, &launches, nullptr)
+                             : hexdyn_strict::run_step(c, s_in, d_in, s_out, d_out, st, &launches, nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "no-alloc step");
+  int flag = 0;
+  HEX_CUDA(cudaMemcpyAsync(&flag, c.w.flag, sizeof(int), cudaMemcpyDeviceToHost, st), "flag D2H");
+  HEX_CUDA(cudaStreamSynchronize(st), "no-alloc step sync");
+  if (flag_out) *flag_out = flag;
+  if (flag) return fail(HEXDYN_E_NUMERIC, "device validation flag 0x%x set in the no-alloc step", flag);
+  return HEXDYN_OK;
+}
+

@@ -30,6 +30,12 @@ _I32P = C.POINTER(C.c_int32)
 _F32P = C.POINTER(C.c_float)
 
 
+class HexDynFields(C.Structure):
+    """Device pointers of one state + sidecar, indexed by FIELDS values."""
+
+    _fields_ = [("field", C.c_void_p * 12)]
+
+
 class HexDynDesc(C.Structure):
     _fields_ = [
         ("n_cells", C.c_int32), ("n_edges", C.c_int32), ("n_vertices", C.c_int32), ("n_levels", C.c_int32),
@@ -71,6 +77,8 @@ EXPORTS = {
     "hexdyn_level_stride": (C.c_int, [C.c_void_p]),
     "hexdyn_launches_per_step": (C.c_longlong, [C.c_void_p]),
     "hexdyn_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "hexdyn_step_noalloc": (C.c_int, [C.c_void_p, C.POINTER(HexDynFields), C.POINTER(HexDynFields),
+                                      C.c_void_p, C.POINTER(C.c_int)]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -169,6 +169,35 @@ int hexdyn_level_stride(HexDynHandle* h);
 long long hexdyn_launches_per_step(HexDynHandle* h);
 size_t hexdyn_device_bytes(HexDynHandle* h);
 
+/* Caller-owned device buffers of one state and sidecar, in the library's
+ * padded [entity][level] layout (level stride from hexdyn_level_stride;
+ * scalars [tracer][cell][level]), indexed by HexDynField. */
+typedef struct HexDynFields {
+  float* field[HEXDYN_NUM_FIELDS];
+} HexDynFields;
+
+/* No counterpart in the reference: one large step that allocates nothing.
+ * For callers that cannot call cudaMalloc when they step -- code running
+ * while its own stream is being captured into a CUDA graph (an allocation
+ * there breaks the capture), host frameworks whose device memory is owned by
+ * a pool that must not be bypassed, or ensembles that keep every member's
+ * state in their own buffers and cannot give each member a private
+ * workspace.  The caller passes the input state and sidecar and the output
+ * buffers (`in` and `out` must not overlap); the mesh comes from `h`.  Every
+ * intermediate of the step (tendencies, acoustic perturbations, coefficients,
+ * subcycle states, transport limiter fields) lives in one file-scope device
+ * array of 64 MiB that each GPU loading the library holds until exit; a step
+ * needing more returns HEXDYN_E_CAPACITY and names the size.  The first call
+ * on a device looks up that array's address (cudaGetSymbolAddress) and must
+ * come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (different streams, or concurrent host threads) race on
+ * it, so issue them on one stream.  Each call clears what must start at zero
+ * (the validation flag and the dry moist-coefficient fields) and writes every
+ * other scratch word before reading it.  Reads the flag at the end like
+ * hexdyn_step (synchronises `stream`). */
+int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, const HexDynFields* out, void* stream,
+                        int* flag_out);
+
 /* Copy the last error message of this thread into buf. */
 int hexdyn_last_error(char* buf, size_t len);
 

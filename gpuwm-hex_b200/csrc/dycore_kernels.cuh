@@ -577,7 +577,11 @@ __global__ void k_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float 
 // One acoustic cell pass (hexcore/acoustic_v841.py:461-567): rs/ts from the
 // edge fluxes of ru_p, the rw_p right-hand side, the dts^2 Thomas sweep
 // (:236-257, one thread per column, levels in order), implicit Rayleigh
-// damping, ww_avg, and the rho_pp / rtheta_pp updates.
+// damping, ww_avg, and the rho_pp / rtheta_pp updates.  Everything the
+// sequential sweep reads (rhs, dts2*a, alpha, gamma) is staged in shared
+// memory by the level-parallel phase first, so the recurrence never waits
+// on a global load.
+#define HEX_AC_SMEM_ARRAYS 8
 __global__ void k_ac_cell(HexGeo g, int first, float dts, float dts2, const float* __restrict__ ru_p,
                           const float* __restrict__ theta_s, const float* __restrict__ tend_rho,
                           const float* __restrict__ tend_rt, const float* __restrict__ tend_rw,
@@ -594,11 +598,14 @@ __global__ void k_ac_cell(HexGeo g, int first, float dts, float dts2, const floa
   const int S = g.S, L = g.L;
   const int c = blockIdx.x * blockDim.y + threadIdx.y;
   const bool live = c < g.nC;
-  float* s_rs = sm + threadIdx.y * S * 5;
+  float* s_rs = sm + threadIdx.y * S * HEX_AC_SMEM_ARRAYS;
   float* s_ts = s_rs + S;
   float* s_rho = s_ts + S;
   float* s_rt = s_rho + S;
   float* s_r = s_rt + S;
+  float* s_da = s_r + S;
+  float* s_al = s_da + S;
+  float* s_ga = s_al + S;
   const int i = c * S + k;
   const float* ewm = g.ewm;
   const float* ewp = g.ewp;
@@ -608,6 +615,11 @@ __global__ void k_ac_cell(HexGeo g, int first, float dts, float dts2, const floa
   if (live) {
     if (k <= L) rwp_old = first ? 0.0f : rw_p[i];
     s_r[k] = rwp_old;
+    if (k < L) {
+      s_da[k] = dts2 * a_tri[i];
+      s_al[k] = alpha_tri[i];
+      s_ga[k] = gamma_tri[i];
+    }
   }
   __syncthreads();
   if (live) {
@@ -651,17 +663,16 @@ __global__ void k_ac_cell(HexGeo g, int first, float dts, float dts2, const floa
   if (live && k <= L) s_r[k] = rhs;
   __syncthreads();
   if (live && k == 0) {
-    const float* a = a_tri + c * S;
-    const float* al = alpha_tri + c * S;
-    const float* ga = gamma_tri + c * S;
     float prev = s_r[0];
+#pragma unroll 4
     for (int kk = 1; kk < L; ++kk) {
-      prev = (s_r[kk] - dts2 * a[kk] * prev) * al[kk];
+      prev = (s_r[kk] - s_da[kk] * prev) * s_al[kk];
       s_r[kk] = prev;
     }
     float next = s_r[L];
+#pragma unroll 4
     for (int kk = L - 1; kk >= 0; --kk) {
-      next = s_r[kk] - ga[kk] * next;
+      next = s_r[kk] - s_ga[kk] * next;
       s_r[kk] = next;
     }
   }

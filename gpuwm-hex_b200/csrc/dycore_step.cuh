@@ -64,7 +64,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   const HexGeo& g = ctx.geo;
   HexWork& w = ctx.w;
   const int nT = ctx.n_scalars;
-  const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * 5;
+  const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * HEX_AC_SMEM_ARRAYS;
 
   if (g.moist) {
     LP(L, g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);

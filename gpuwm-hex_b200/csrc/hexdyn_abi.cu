@@ -221,6 +221,9 @@ int validate(const HexDynDesc* d) {
     return fail(HEXDYN_E_ARG, "n_levels=%d: the third-order vertical fluxes need at least 4 levels", d->n_levels);
   if (d->max_edges <= 0 || d->max_edges2 <= 0 || d->adv_width <= 0 || d->n_scalars < 0)
     return fail(HEXDYN_E_ARG, "invalid slot widths or scalar count");
+  if (d->max_edges > 8 || d->max_edges2 > 16 || d->adv_width > 16)
+    return fail(HEXDYN_E_ARG, "slot widths (maxEdges %d, maxEdges2 %d, advection stencil %d) exceed the "
+                "compiled maxima 8 / 16 / 16", d->max_edges, d->max_edges2, d->adv_width);
   if (!(d->dt > 0.0) || !isfinite(d->dt)) return fail(HEXDYN_E_ARG, "config_dt=%g must be finite and positive", d->dt);
   if (d->n_sub_steps < 1) return fail(HEXDYN_E_ARG, "config_number_of_sub_steps=%d must be positive", d->n_sub_steps);
   if (d->split_steps != 1 && d->split_steps != 3)

@@ -75,6 +75,7 @@ struct HexGeo {
   float smdiv_base;   // 2*smdiv*len_disp in FP32 operations
   int apvm_on;
   int moist;          // 0 = dry coefficients, 1 = native (all scalars load)
+  int winds_zero;     // u_init and v_init are zero at every level
 };
 
 #define HEX_FLAG_DENSITY 1

@@ -1,0 +1,986 @@
+// Level-vector kernels: each thread owns four consecutive levels of one
+// entity and moves them with 128-bit loads and stores.  The [entity][level]
+// layout with a stride S that is a multiple of 8 makes every 4-level chunk
+// 16-byte aligned.  Per-level arithmetic is exactly the scalar kernels'
+// (the reference's order); only the data movement is vectorised, so the
+// index loads, coefficient loads and address arithmetic of an entity are
+// shared by four levels and each thread carries four independent chains.
+//
+// Thread layout: blockDim = (S/4, EPB4); x selects the chunk k0 = 4*x.
+
+#define HEX_VEC_PARALLEL(n)                                \
+  const int k0 = threadIdx.x * 4;                          \
+  const int ent = blockIdx.x * blockDim.y + threadIdx.y;   \
+  if (ent >= (n)) return;
+
+struct V4 {
+  float a[4];
+};
+
+__device__ __forceinline__ V4 v4zero() { return V4{{0.0f, 0.0f, 0.0f, 0.0f}}; }
+
+// read-only (non-coherent) 128-bit load: the array is not written by the kernel
+__device__ __forceinline__ V4 ld4(const float* __restrict__ p) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+  return V4{{t.x, t.y, t.z, t.w}};
+}
+// coherent 128-bit load for arrays the kernel also writes
+__device__ __forceinline__ V4 ld4rw(const float* p) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  return V4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ void st4(float* p, const V4& v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
+}
+// Store the lanes whose level k0+j lies in [lo, hi): the levels the
+// one-level-per-thread form of the kernel writes; other words are untouched.
+__device__ __forceinline__ void st4m(float* p, const V4& v, int k0, int lo, int hi) {
+  if (k0 >= lo && k0 + 4 <= hi) {
+    st4(p, v);
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (k0 + j >= lo && k0 + j < hi) p[j] = v.a[j];
+}
+
+// Column window col[k0-4 .. k0+7] around a thread's chunk; entries outside
+// [0, S) read as zero and are never used by a formula.
+struct Win {
+  float a[12];
+  __device__ __forceinline__ float operator()(int d) const { return a[d + 4]; }
+};
+__device__ __forceinline__ Win win(const float* __restrict__ col, int k0, int S) {
+  Win w;
+  const V4 m = ld4(col + k0);
+  const V4 lo = k0 >= 4 ? ld4(col + k0 - 4) : v4zero();
+  const V4 hi = k0 + 4 < S ? ld4(col + k0 + 4) : v4zero();
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    w.a[j] = lo.a[j];
+    w.a[j + 4] = m.a[j];
+    w.a[j + 8] = hi.a[j];
+  }
+  return w;
+}
+
+// ---------------------------------------------------------- diagnostics
+// hexcore/diagnostics.py:95 compute_solve_diagnostics, v8.4.1 stored inverses.
+
+__global__ void kv_diag_vertex(HexGeo g, const float* __restrict__ u, float* __restrict__ pv_vertex,
+                               float* __restrict__ ke_vertex) {
+  HEX_VEC_PARALLEL(g.nV)
+  const int v = ent, S = g.S;
+  V4 vort = v4zero(), ke[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int e = g.eov[3 * v + s];
+    const float vd = g.vsign[3 * v + s] * g.dc[e];
+    const float dd = g.dc[e] * g.dv[e];
+    const V4 ue = ld4(u + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      vort.a[j] = vort.a[j] + vd * ue.a[j];
+      ke[s].a[j] = dd * (ue.a[j] * ue.a[j]);
+    }
+  }
+  const float ia = g.inv_area_tri[v], r = 0.25f * g.inv_area_tri[v], f = g.f_vertex[v];
+  V4 pv, kv;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    pv.a[j] = f + vort.a[j] * ia;
+    kv.a[j] = (ke[0].a[j] + ke[1].a[j] + ke[2].a[j]) * r;
+  }
+  st4m(pv_vertex + v * S + k0, pv, k0, 0, g.L);
+  st4m(ke_vertex + v * S + k0, kv, k0, 0, g.L);
+}
+
+__global__ void kv_diag_cell(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
+                             const float* __restrict__ ke_vertex, float* __restrict__ ke_out,
+                             float* __restrict__ pv_cell) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const int n = g.deg[c];
+  const float ia = g.inv_area[c];
+  V4 ke = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float dd = g.dc[e] * g.dv[e];
+    const V4 ue = ld4(u + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] + 0.25f * (dd * (ue.a[j] * ue.a[j]));
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] * ia * 0.625f;
+  for (int s = 0; s < n; ++s) {
+    const int vtx = g.voc[c * g.maxE + s];
+    const float kt = (1.0f - 0.625f) * g.kite[3 * vtx + g.kite_slot[c * g.maxE + s]];
+    const V4 kv = ld4(ke_vertex + vtx * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] + kt * kv.a[j] * ia;
+  }
+  st4m(ke_out + c * S + k0, ke, k0, 0, g.L);
+  if (g.apvm_on) {
+    V4 pvc = v4zero();
+    for (int s = 0; s < n; ++s) {
+      const int vtx = g.voc[c * g.maxE + s];
+      const float kite = g.kite[3 * vtx + g.kite_slot[c * g.maxE + s]];
+      const V4 pv = ld4(pv_vertex + vtx * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pvc.a[j] = pvc.a[j] + kite * pv.a[j] * ia;
+    }
+    st4m(pv_cell + c * S + k0, pvc, k0, 0, g.L);
+  }
+}
+
+__global__ void kv_diag_edge(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
+                             const float* __restrict__ pv_cell, float* __restrict__ v, float* __restrict__ pv_edge,
+                             int recompute_v) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  V4 vt;
+  if (recompute_v) {
+    vt = v4zero();
+    const int n = g.neoe[e];
+    for (int s = 0; s < n; ++s) {
+      const float w = g.weights[e * g.maxE2 + s];
+      const V4 un = ld4(u + g.eoe[e * g.maxE2 + s] * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) vt.a[j] = vt.a[j] + w * un.a[j];
+    }
+    st4m(v + e * S + k0, vt, k0, 0, g.L);
+  } else {
+    vt = ld4rw(v + e * S + k0);
+  }
+  const int v0 = g.voe[2 * e], v1 = g.voe[2 * e + 1];
+  const V4 p0 = ld4(pv_vertex + v0 * S + k0), p1 = ld4(pv_vertex + v1 * S + k0);
+  V4 pve;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) pve.a[j] = 0.5f * (p0.a[j] + p1.a[j]);
+  if (g.apvm_on) {
+    const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+    const V4 q0 = ld4(pv_cell + c0 * S + k0), q1 = ld4(pv_cell + c1 * S + k0);
+    const V4 ue = ld4(u + e * S + k0);
+    const float idv = g.inv_dv[e], idc = g.inv_dc[e];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float gpt = (p1.a[j] - p0.a[j]) * idv;
+      const float gpn = (q1.a[j] - q0.a[j]) * idc;
+      pve.a[j] = pve.a[j] - g.apvm_scale * (vt.a[j] * gpt + ue.a[j] * gpn);
+    }
+  }
+  st4m(pv_edge + e * S + k0, pve, k0, 0, g.L);
+}
+
+// --------------------------------------------------------- Euler terms
+
+__device__ __forceinline__ float dpdz_of(const HexGeo& g, float rp, float qt, float rb) {
+  if (!g.moist) return -g.g * rp;
+  return -g.g * (rb * qt + rp * (1.0f + qt));
+}
+
+// hexcore/dynamics.py:188 pressure_gradient_euler_tendency.
+__global__ void kv_euler_edge(HexGeo g, const float* __restrict__ pp, const float* __restrict__ rp,
+                              const float* __restrict__ qtot, const float* __restrict__ cqu,
+                              float* __restrict__ euler_ru) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  const V4 p0 = ld4(pp + i0), p1 = ld4(pp + i1), r0 = ld4(rp + i0), r1 = ld4(rp + i1);
+  // moisture terms of dpdz are read only with native moist coefficients
+  const bool m = g.moist;
+  const V4 q0 = m ? ld4(qtot + i0) : v4zero(), q1 = m ? ld4(qtot + i1) : v4zero();
+  const V4 b0 = m ? ld4(g.rho_base + i0) : v4zero(), b1 = m ? ld4(g.rho_base + i1) : v4zero();
+  const V4 z0 = ld4(g.zz + i0), z1 = ld4(g.zz + i1);
+  const V4 cq = ld4(cqu + e * S + k0), zx = ld4(g.zxu + e * S + k0);
+  const float idc = g.inv_dc[e];
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float d0 = dpdz_of(g, r0.a[j], q0.a[j], b0.a[j]);
+    const float d1 = dpdz_of(g, r1.a[j], q1.a[j], b1.a[j]);
+    out.a[j] = -cq.a[j] * ((p1.a[j] - p0.a[j]) * idc / (0.5f * (z1.a[j] + z0.a[j])) - 0.5f * zx.a[j] * (d0 + d1));
+  }
+  st4m(euler_ru + e * S + k0, out, k0, 0, g.L);
+}
+
+// hexcore/dynamics.py:86 mass_flux_divergence (stored inverse area), 4 levels.
+__device__ __forceinline__ V4 mass_flux_div4(const HexGeo& g, const float* __restrict__ ru, int c, int k0) {
+  V4 acc = v4zero();
+  const int n = g.deg[c];
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float sd = g.csign[c * g.maxE + s] * g.dv[e];
+    const V4 r = ld4(ru + e * g.S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] + sd * r.a[j];
+  }
+  const float ia = g.inv_area[c];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] * ia;
+  return acc;
+}
+
+// hexcore/dynamics.py:122 density_tendency and hexcore/driver.py:2804 Euler w.
+__global__ void kv_euler_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ rw,
+                              const float* __restrict__ pp, const float* __restrict__ rp,
+                              const float* __restrict__ qtot, const float* __restrict__ cqw,
+                              float* __restrict__ tend_rho, float* __restrict__ euler_rw) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const V4 hd = mass_flux_div4(g, ru, c, k0);
+  const Win rww = win(rw + c * S, k0, S);
+  const Win ppw = win(pp + c * S, k0, S), rpw = win(rp + c * S, k0, S);
+  const bool m = g.moist;
+  const Win qtw = m ? win(qtot + c * S, k0, S) : Win{}, rbw = m ? win(g.rho_base + c * S, k0, S) : Win{};
+  const V4 cq = m ? ld4(cqw + c * S + k0) : v4zero();
+  V4 tr, er;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    tr.a[j] = -hd.a[j] - g.rdzw[k] * (rww(j + 1) - rww(j));
+    float out = 0.0f;
+    if (k >= 1 && k < L) {
+      const float dk = dpdz_of(g, rpw(j), qtw(j), rbw(j));
+      const float dm = dpdz_of(g, rpw(j - 1), qtw(j - 1), rbw(j - 1));
+      const float inner = g.rdzu[k] * (ppw(j) - ppw(j - 1)) - (g.fzm[k] * dk + g.fzp[k] * dm);
+      out = m ? -(cq.a[j] * inner) : -inner;
+    }
+    er.a[j] = out;
+  }
+  st4m(tend_rho + c * S + k0, tr, k0, 0, g.L);
+  st4m(euler_rw + c * S + k0, er, k0, 0, g.L + 1);
+}
+
+// ------------------------------------------------- stage tendencies
+
+__global__ void kv_hdiv(HexGeo g, const float* __restrict__ ru, float* __restrict__ hdiv) {
+  HEX_VEC_PARALLEL(g.nC)
+  st4m(hdiv + ent * g.S + k0, mass_flux_div4(g, ru, ent, k0), k0, 0, g.L);
+}
+
+// Third-order edge values of theta_m (levels) and w (interfaces):
+// hexcore/driver.py:1023-1034 and :1159-1172.
+__global__ void kv_edge_adv(HexGeo g, const float* __restrict__ ru, const float* __restrict__ theta,
+                            const float* __restrict__ w, float* __restrict__ edge_theta,
+                            float* __restrict__ edge_w) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int n = g.n_adv[e];
+  const int* cells = g.adv_cells + (size_t)e * g.advW;
+  const float* a1 = g.adv + (size_t)e * g.advW;
+  const float* a3 = g.adv3 + (size_t)e * g.advW;
+  const V4 r = ld4(ru + e * S + k0);
+  const float rm = k0 > 0 ? ru[e * S + k0 - 1] : 0.0f;
+  float ct[4], cw[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    ct[j] = g.coef3 * copysignf(1.0f, r.a[j]);
+    const float rprev = j == 0 ? rm : r.a[j - 1];
+    const float rui = g.fzm[k] * r.a[j] + g.fzp[k] * rprev;
+    cw[j] = g.coef3 * copysignf(1.0f, rui);
+  }
+  V4 at = v4zero(), aw = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int cs = cells[s] * S + k0;
+    const float A = a1[s], B = a3[s];
+    const V4 th = ld4(theta + cs), wv = ld4(w + cs);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      at.a[j] = at.a[j] + (A + ct[j] * B) * th.a[j];
+      aw.a[j] = aw.a[j] + (A + cw[j] * B) * wv.a[j];
+    }
+  }
+  st4m(edge_theta + e * S + k0, at, k0, 0, g.L);
+  st4m(edge_w + e * S + k0, aw, k0, 1, g.L);
+}
+
+// wduz at interface j of the edge (hexcore/dynamics.py:227), from windows of
+// u (edge) and rw at both cells; d = j - k0 in [0, 4].
+__device__ __forceinline__ float wduz_win(const HexGeo& g, const Win& uw, const Win& r0, const Win& r1, int k0,
+                                          int d) {
+  const int j = k0 + d, L = g.L;
+  if (j <= 0 || j >= L) return 0.0f;
+  const float rwe = 0.5f * (r0(d) + r1(d));
+  if (j == 1 || j == L - 1) return rwe * (g.fzm[j] * uw(d) + g.fzp[j] * uw(d - 1));
+  return flux3f(uw(d - 2), uw(d - 1), uw(d), uw(d + 1), rwe, 1.0f);
+}
+
+// tend_ru: vertical transport + hexcore/dynamics_v841.py:121 momentum + saved Euler.
+__global__ void kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
+                          const float* __restrict__ rho, const float* __restrict__ pv_edge,
+                          const float* __restrict__ ke, const float* __restrict__ hdiv,
+                          const float* __restrict__ euler_ru, float* __restrict__ tend_ru) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+  const Win uw = win(u + e * S, k0, S);
+  const Win r0 = win(rw + c0 * S, k0, S), r1 = win(rw + c1 * S, k0, S);
+  float wd[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) wd[d] = wduz_win(g, uw, r0, r1, k0, d);
+  const int n = g.neoe[e];
+  const V4 pve = ld4(pv_edge + e * S + k0);
+  V4 q = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int nb = g.eoe[e * g.maxE2 + s];
+    const float w = g.weights[e * g.maxE2 + s];
+    const V4 un = ld4(u + nb * S + k0), pn = ld4(pv_edge + nb * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float work_pv = 0.5f * (pve.a[j] + pn.a[j]);
+      q.a[j] = q.a[j] + w * un.a[j] * work_pv;
+    }
+  }
+  // Perturbation-Coriolis subtraction.  With all-zero reference winds every
+  // subtracted term is a signed zero, and q - (+-0) == q bit for bit unless
+  // q is itself zero or NaN, so the loop runs only when it can change a bit.
+  bool need = !g.winds_zero;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) need = need || !(fabsf(q.a[j]) > 0.0f);
+  if (need) {
+    const float fe = g.f_edge[e];
+    for (int s = 0; s < n; ++s) {
+      const int nb = g.eoe[e * g.maxE2 + s];
+      const float w = g.weights[e * g.maxE2 + s];
+      const float ca = g.cos_angle[nb], sa = g.sin_angle[nb];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        const float ref_u = g.u_init[k] * ca - g.v_init[k] * sa;
+        q.a[j] = q.a[j] - w * ref_u * fe;
+      }
+    }
+  }
+  const V4 rh0 = ld4(rho + c0 * S + k0), rh1 = ld4(rho + c1 * S + k0);
+  const V4 ke0 = ld4(ke + c0 * S + k0), ke1 = ld4(ke + c1 * S + k0);
+  const V4 hd0 = ld4(hdiv + c0 * S + k0), hd1 = ld4(hdiv + c1 * S + k0);
+  const V4 eu = ld4(euler_ru + e * S + k0);
+  const float idc = g.inv_dc[e];
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    const float tv = -g.rdzw[k] * (wd[j + 1] - wd[j]);
+    const float rho_edge = 0.5f * (rh0.a[j] + rh1.a[j]);
+    float horizontal = rho_edge * (q.a[j] - (ke1.a[j] - ke0.a[j]) * idc);
+    horizontal = tv + horizontal;
+    const float res = horizontal - uw(j) * 0.5f * (hd0.a[j] + hd1.a[j]);
+    out.a[j] = res + eu.a[j];
+  }
+  st4m(tend_ru + e * S + k0, out, k0, 0, g.L);
+}
+
+// theta vertical flux at interface j = k0 + d (hexcore/driver.py:1048-1076).
+__device__ __forceinline__ float vflux_theta_win(const HexGeo& g, const Win& th, const Win& ths, const Win& rw,
+                                                 const Win& rws, int k0, int d) {
+  const int j = k0 + d, L = g.L;
+  if (j <= 0 || j >= L) return 0.0f;
+  if (j == 1) {
+    const float vf = rw(d) * (g.fzm[j] * th(d) + g.fzp[j] * th(d - 1));
+    return vf + (rws(d) - rw(d)) * (g.fzm[j] * ths(d) + g.fzp[j] * ths(d - 1));
+  }
+  if (j == L - 1) return rws(d) * (g.fzm[j] * th(d) + g.fzp[j] * th(d - 1));
+  const float vf = flux3f(th(d - 2), th(d - 1), th(d), th(d + 1), rw(d), g.coef3);
+  return vf + (rws(d) - rw(d)) * (g.fzm[j] * ths(d) + g.fzp[j] * ths(d - 1));
+}
+
+// w vertical flux at interface j = k0 + d (hexcore/driver.py:1176-1200).
+__device__ __forceinline__ float vflux_w_win(const HexGeo& g, const Win& w, const Win& rw, int k0, int d) {
+  const int j = k0 + d, L = g.L;
+  if (j <= 0 || j >= L) return 0.0f;
+  if (j == 1 || j == L - 1) return 0.25f * (rw(d) + rw(d - 1)) * (w(d) + w(d - 1));
+  return flux3f(w(d - 2), w(d - 1), w(d), w(d + 1), 0.5f * (rw(d) + rw(d - 1)), 1.0f);
+}
+
+// tend_rt (hexcore/driver.py:933), tend_rw (:1081) + Euler w, then
+// hexcore/acoustic.py:246 convert_w_tendency_to_omega.
+__global__ void kv_tend_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ ru_s,
+                             const float* __restrict__ rw, const float* __restrict__ rws,
+                             const float* __restrict__ theta, const float* __restrict__ theta_s,
+                             const float* __restrict__ w, const float* __restrict__ edge_theta,
+                             const float* __restrict__ edge_w, const float* __restrict__ euler_rw,
+                             const float* __restrict__ tend_ru, float* __restrict__ tend_rt,
+                             float* __restrict__ tend_rw, int rk_step) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const int n = g.deg[c];
+  const float ia = g.inv_area[c];
+  const int* eoc = g.eoc + c * g.maxE;
+  const float* cs = g.csign + c * g.maxE;
+  // horizontal parts: rho-theta flux divergence, RK>1 correction, w flux
+  V4 res = v4zero(), hres = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int e = eoc[s];
+    const float sg = cs[s];
+    const V4 r = ld4(ru + e * S + k0), et = ld4(edge_theta + e * S + k0), ew = ld4(edge_w + e * S + k0);
+    const float rm = k0 > 0 ? ru[e * S + k0 - 1] : 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      res.a[j] = res.a[j] - sg * r.a[j] * et.a[j];
+      const float rprev = j == 0 ? rm : r.a[j - 1];
+      const float rui = g.fzm[k] * r.a[j] + g.fzp[k] * rprev;
+      hres.a[j] = hres.a[j] - sg * rui * ew.a[j];
+    }
+  }
+  if (rk_step > 1) {
+    for (int s = 0; s < n; ++s) {
+      const int e = eoc[s];
+      const int e0 = g.coe[2 * e], e1 = g.coe[2 * e + 1];
+      const float dvs = cs[s] * g.dv[e];
+      const V4 r = ld4(ru + e * S + k0), rs = ld4(ru_s + e * S + k0);
+      const V4 t1 = ld4(theta_s + e1 * S + k0), t0 = ld4(theta_s + e0 * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float corr = dvs * (rs.a[j] - r.a[j]) * 0.5f * (t1.a[j] + t0.a[j]);
+        res.a[j] = res.a[j] - corr;
+      }
+    }
+  }
+  const Win th = win(theta + c * S, k0, S), ths = win(theta_s + c * S, k0, S);
+  const Win rww = win(rw + c * S, k0, S), rwsw = win(rws + c * S, k0, S);
+  const Win ww = win(w + c * S, k0, S), zzw = win(g.zz + c * S, k0, S);
+  const V4 er = ld4(euler_rw + c * S + k0);
+  float vt[5], vw[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    vt[d] = vflux_theta_win(g, th, ths, rww, rwsw, k0, d);
+    vw[d] = vflux_w_win(g, ww, rww, k0, d);
+  }
+  V4 trt, trw;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    trt.a[j] = res.a[j] * ia - g.rdzw[k] * (vt[j + 1] - vt[j]);
+    if (k >= 1 && k < L) {
+      const float rsw = hres.a[j] * ia - g.rdzu[k] * (vw[j + 1] - vw[j]);
+      trw.a[j] = rsw + er.a[j];
+    } else {
+      trw.a[j] = 0.0f + er.a[j];
+    }
+  }
+  // omega conversion (interfaces 1..L-1)
+  for (int s = 0; s < n; ++s) {
+    const int e = eoc[s];
+    const float sg = cs[s];
+    const V4 t = ld4(tend_ru + e * S + k0);
+    const float tm = k0 > 0 ? tend_ru[e * S + k0 - 1] : 0.0f;
+    const int zi = (c * g.maxE + s) * S + k0;
+    const V4 zb = ld4(g.zb + zi), zb3 = ld4(g.zb3 + zi);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      if (k >= 1 && k < L) {
+        const float tprev = j == 0 ? tm : t.a[j - 1];
+        const float flux = sg * (g.fzm[k] * t.a[j] + g.fzp[k] * tprev);
+        const float up = copysignf(1.0f, t.a[j]);
+        trw.a[j] = trw.a[j] - (zb.a[j] + up * zb3.a[j]) * flux;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    if (k >= 1 && k < L) trw.a[j] = trw.a[j] * (g.fzm[k] * zzw(j) + g.fzp[k] * zzw(j - 1));
+    if (k > L) trw.a[j] = 0.0f;
+  }
+  st4m(tend_rt + c * S + k0, trt, k0, 0, g.L);
+  st4m(tend_rw + c * S + k0, trw, k0, 0, g.L + 1);
+}
+
+// ------------------------------------------------------------- acoustic
+
+// One acoustic edge pass (see k_ac_edge): mode 0 first substep, 1 damping of
+// the previous substep + update, 2 damping only.
+__global__ void kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float damp_coef,
+                           const float* __restrict__ tend_ru, const float* __restrict__ rtpp_new,
+                           const float* __restrict__ rtpp_old, const float* __restrict__ rho_pp,
+                           const float* __restrict__ theta_s, const float* __restrict__ exner_s,
+                           const float* __restrict__ cqu, float* __restrict__ ru_p, float* __restrict__ ru_avg) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int jj = e * S + k0;
+  if (mode == 0) {
+    const V4 t = ld4(tend_ru + jj);
+    V4 r;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) r.a[j] = dts * t.a[j];
+    st4m(ru_p + jj, r, k0, 0, g.L);
+    st4m(ru_avg + jj, r, k0, 0, g.L);
+    return;
+  }
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  V4 r = ld4rw(ru_p + jj);
+  const V4 n0 = ld4(rtpp_new + i0), n1 = ld4(rtpp_new + i1);
+  const V4 o0 = old_is_zero ? v4zero() : ld4(rtpp_old + i0);
+  const V4 o1 = old_is_zero ? v4zero() : ld4(rtpp_old + i1);
+  const V4 t0 = ld4(theta_s + i0), t1 = ld4(theta_s + i1);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float d0 = n0.a[j] - o0.a[j];
+    const float d1 = n1.a[j] - o1.a[j];
+    r.a[j] = r.a[j] + damp_coef * (d0 - d1) * (1.0f - 0.0f) / (t0.a[j] + t1.a[j]);
+  }
+  if (mode == 1) {
+    const V4 z0 = ld4(g.zz + i0), z1 = ld4(g.zz + i1), x0 = ld4(exner_s + i0), x1 = ld4(exner_s + i1);
+    const V4 p0 = ld4(rho_pp + i0), p1 = ld4(rho_pp + i1);
+    const V4 cq = ld4(cqu + jj), zx = ld4(g.zxu + jj), t = ld4(tend_ru + jj);
+    V4 av = ld4rw(ru_avg + jj);
+    const float idc = g.inv_dc[e];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float pg = (n1.a[j] - n0.a[j]) * idc / (0.5f * (z1.a[j] + z0.a[j]));
+      pg = cq.a[j] * 0.5f * g.c2 * (x0.a[j] + x1.a[j]) * pg;
+      pg = pg + 0.5f * zx.a[j] * g.g * (p0.a[j] + p1.a[j]);
+      r.a[j] = r.a[j] + dts * (t.a[j] - pg);
+      av.a[j] = av.a[j] + r.a[j];
+    }
+    st4m(ru_avg + jj, av, k0, 0, g.L);
+  }
+  st4m(ru_p + jj, r, k0, 0, g.L);
+}
+
+// ---------------------------------------------------------- stage recovery
+
+__global__ void kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, const float* __restrict__ ru_p,
+                                const float* __restrict__ ru_avg, const float* __restrict__ rp_s,
+                                const float* __restrict__ rho_pp, float* __restrict__ ru_out,
+                                float* __restrict__ u_out, float* __restrict__ flux_u, int flux_mode,
+                                float inv_steps, float inv_splits) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int jj = e * S + k0;
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  const V4 a0 = ld4(rp_s + i0), a1 = ld4(rp_s + i1), b0 = ld4(rho_pp + i0), b1 = ld4(rho_pp + i1);
+  const V4 c0 = ld4(g.rho_base + i0), c1 = ld4(g.rho_base + i1);
+  const V4 rs = ld4(ru_s + jj), rp = ld4(ru_p + jj);
+  V4 ru, uo;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float rho0 = a0.a[j] + b0.a[j] + c0.a[j];
+    const float rho1 = a1.a[j] + b1.a[j] + c1.a[j];
+    ru.a[j] = rs.a[j] + rp.a[j];
+    uo.a[j] = 2.0f * ru.a[j] / (rho0 + rho1);
+  }
+  st4m(ru_out + jj, ru, k0, 0, g.L);
+  st4m(u_out + jj, uo, k0, 0, g.L);
+  if (flux_mode & 4) {
+    const V4 av = ld4(ru_avg + jj);
+    const V4 old = (flux_mode & 1) ? v4zero() : ld4rw(flux_u + jj);
+    V4 acc;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float f = rs.a[j] + av.a[j] * inv_steps;
+      float a = (flux_mode & 1) ? f : f + old.a[j];
+      if (flux_mode & 2) a = a * inv_splits;
+      acc.a[j] = a;
+    }
+    st4m(flux_u + jj, acc, k0, 0, g.L);
+  }
+}
+
+__global__ void kv_recover_cell(HexGeo g, int stage3, const float* __restrict__ rp_s,
+                                const float* __restrict__ rtp_s, const float* __restrict__ rw_s,
+                                const float* __restrict__ rho_pp, const float* __restrict__ rtpp,
+                                const float* __restrict__ rw_p, const float* __restrict__ ww_avg,
+                                const float* __restrict__ ru_new, HexState out, HexSide side,
+                                float* __restrict__ flux_w, int flux_mode, float inv_steps, float inv_splits,
+                                int* flag) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const int ii = c * S + k0;
+  // candidate density on the window k0-4 .. k0+7 (recomputed, not read back)
+  const Win rpw = win(rp_s + c * S, k0, S), ppw = win(rho_pp + c * S, k0, S), rbw = win(g.rho_base + c * S, k0, S);
+  float rho_w[12];
+#pragma unroll
+  for (int d = -4; d < 8; ++d) rho_w[d + 4] = rpw(d) + ppw(d) + rbw(d);
+  {
+    const V4 tp = ld4(rtp_s + ii), tq = ld4(rtpp + ii), tb = ld4(g.rtheta_base + ii);
+    V4 rho, rt, rp, rtp, th;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      rp.a[j] = rpw(j) + ppw(j);
+      rtp.a[j] = tp.a[j] + tq.a[j];
+      rho.a[j] = rp.a[j] + rbw(j);
+      rt.a[j] = rtp.a[j] + tb.a[j];
+      th.a[j] = rt.a[j] / rho.a[j];
+      if (k0 + j < L && (!(rho.a[j] > 0.0f) || !(rt.a[j] > 0.0f))) bad = true;
+    }
+    if (bad) atomicOr(flag, HEX_FLAG_DENSITY);
+    st4m(out.rho + ii, rho, k0, 0, g.L);
+    st4m(out.rho_theta + ii, rt, k0, 0, g.L);
+    st4m(side.rho_p + ii, rp, k0, 0, g.L);
+    st4m(side.rtheta_p + ii, rtp, k0, 0, g.L);
+    st4m(side.theta_m + ii, th, k0, 0, g.L);
+    if (stage3) {
+      const V4 zz = ld4(g.zz + ii), eb = ld4(g.exner_base + ii);
+      V4 ex, pp;
+      int badp = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (k0 + j < L) {
+          int b = 0;
+          ex.a[j] = hexdyn_powf::powf_gnu(zz.a[j] * g.r_over_p0 * rt.a[j], g.kappa, &b);
+          badp |= b;
+          pp.a[j] = zz.a[j] * g.rgas * (ex.a[j] * rtp.a[j] + tb.a[j] * (ex.a[j] - eb.a[j]));
+        } else {
+          ex.a[j] = 0.0f;
+          pp.a[j] = 0.0f;
+        }
+      }
+      if (badp) atomicOr(flag, HEX_FLAG_POWF);
+      st4m(side.exner + ii, ex, k0, 0, g.L);
+      st4m(side.pressure_p + ii, pp, k0, 0, g.L);
+    }
+  }
+  // rw, w, split flux (interfaces)
+  const V4 rs = ld4(rw_s + ii), rq = ld4(rw_p + ii);
+  V4 rwv, wv;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    rwv.a[j] = (k == 0 || k == L || k > L) ? 0.0f : rs.a[j] + rq.a[j];
+  }
+  st4m(out.rho_w + ii, rwv, k0, 0, g.L + 1);
+  const int n = g.deg[c];
+  const Win zzw = win(g.zz + c * S, k0, S);
+  float acc[4];
+  bool bottom = k0 == 0;
+  float bacc = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    acc[j] = 0.0f;
+    if (k >= 1 && k < L) acc[j] = rwv.a[j] / (g.fzm[k] * zzw(j) + g.fzp[k] * zzw(j - 1));
+  }
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float sign = g.csign[c * g.maxE + s];
+    const V4 r = ld4(ru_new + e * S + k0);
+    const float rm = k0 > 0 ? ru_new[e * S + k0 - 1] : 0.0f;
+    const int zi = (c * g.maxE + s) * S + k0;
+    const V4 zb = ld4(g.zb + zi), zb3 = ld4(g.zb3 + zi);
+    if (bottom) {
+      const float flux = g.cf1 * r.a[0] + g.cf2 * r.a[1] + g.cf3 * r.a[2];
+      bacc = bacc + sign * (zb.a[0] + copysignf(1.0f, flux) * zb3.a[0]) * flux;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      if (k >= 1 && k < L) {
+        const float rprev = j == 0 ? rm : r.a[j - 1];
+        const float flux = g.fzm[k] * r.a[j] + g.fzp[k] * rprev;
+        acc[j] = acc[j] + sign * (zb.a[j] + copysignf(1.0f, flux) * zb3.a[j]) * flux;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    float wk = 0.0f;
+    if (k == 0) {
+      const float bd = g.cf1 * rho_w[4] + g.cf2 * rho_w[5] + g.cf3 * rho_w[6];
+      wk = bacc / bd;
+    } else if (k < L) {
+      const float irho = g.fzm[k] * rho_w[j + 4] + g.fzp[k] * rho_w[j + 3];
+      wk = acc[j] / irho;
+    }
+    wv.a[j] = wk;
+  }
+  st4m(side.w + ii, wv, k0, 0, g.L + 1);
+  if (flux_mode & 4) {
+    const V4 av = ld4(ww_avg + ii);
+    const V4 old = (flux_mode & 1) ? v4zero() : ld4rw(flux_w + ii);
+    V4 fa;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float f = rs.a[j] + av.a[j] * inv_steps;
+      float a = (flux_mode & 1) ? f : f + old.a[j];
+      if (flux_mode & 2) a = a * inv_splits;
+      fa.a[j] = a;
+    }
+    st4m(flux_w + ii, fa, k0, 0, g.L + 1);
+  }
+}
+
+// ------------------------------------------------------------ transport
+
+__global__ void kv_tr_edge(HexGeo g, int mono, const float* __restrict__ q, const float* __restrict__ hv,
+                           float* __restrict__ out) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const float* qt = q + (size_t)blockIdx.z * g.nC * S;
+  const int n = g.n_adv[e];
+  const int* cells = g.adv_cells + (size_t)e * g.advW;
+  const float* a1 = g.adv + (size_t)e * g.advW;
+  const float* a3 = g.adv3 + (size_t)e * g.advW;
+  const V4 vel = ld4(hv + e * S + k0);
+  float cs[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) cs[j] = g.coef3 * copysignf(1.0f, vel.a[j]);
+  V4 res;
+  if (mono && n == 10) {
+    V4 val;
+    {
+      const V4 qv = ld4(qt + cells[0] * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) val.a[j] = (a1[0] + cs[j] * a3[0]) * qv.a[j];
+    }
+    for (int s = 1; s < 10; ++s) {
+      const V4 qv = ld4(qt + cells[s] * S + k0);
+      const float A = a1[s], B = a3[s];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) val.a[j] = val.a[j] + (A + cs[j] * B) * qv.a[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) res.a[j] = vel.a[j] * val.a[j];
+  } else {
+    res = v4zero();
+    for (int s = 0; s < n; ++s) {
+      const V4 qv = ld4(qt + cells[s] * S + k0);
+      const float A = a1[s], B = a3[s];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        float wgt = A + cs[j] * B;
+        if (mono) wgt = vel.a[j] * wgt;
+        res.a[j] = res.a[j] + wgt * qv.a[j];
+      }
+    }
+  }
+  st4m(out + (size_t)blockIdx.z * g.nE * S + e * S + k0, res, k0, 0, g.L);
+}
+
+// transport vertical flux at interface j = k0 + d (hexcore/transport.py:1389).
+__device__ __forceinline__ float tr_vflux_win(const HexGeo& g, const Win& q, const Win& ww, int k0, int d) {
+  const int j = k0 + d, L = g.L;
+  if (j <= 0 || j >= L) return 0.0f;
+  if (j == 1 || j == L - 1) return ww(d) * (g.fzm[j] * q(d) + g.fzp[j] * q(d - 1));
+  const float vel = ww(d);
+  const float base = vel * (7.0f * (q(d) + q(d - 1)) - (q(d + 1) + q(d - 2))) / 12.0f;
+  const float corr = g.coef3 * fabsf(vel) * ((q(d + 1) - q(d - 2)) - 3.0f * (q(d) - q(d - 1))) / 12.0f;
+  return base + corr;
+}
+
+__global__ void kv_tr_std(HexGeo g, float step, float wn, const float* __restrict__ q_old,
+                          const float* __restrict__ q_stage, const float* __restrict__ rho_old,
+                          const float* __restrict__ rho_new, const float* __restrict__ hv,
+                          const float* __restrict__ ww, const float* __restrict__ edge_q,
+                          float* __restrict__ q_out) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const int ii = c * S + k0;
+  const size_t toff = (size_t)blockIdx.z * g.nC * S;
+  const float* ev = edge_q + (size_t)blockIdx.z * g.nE * S;
+  const int n = g.deg[c];
+  V4 t = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float ts = -g.csign[c * g.maxE + s];
+    const V4 h = ld4(hv + e * S + k0), x = ld4(ev + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) t.a[j] = t.a[j] + ts * h.a[j] * x.a[j];
+  }
+  const float ia = g.inv_area[c];
+  const Win qw = win(q_stage + toff + c * S, k0, S), www = win(ww + c * S, k0, S);
+  const V4 ro = ld4(rho_old + ii), rn = ld4(rho_new + ii), qo = ld4(q_old + toff + ii);
+  float vf[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) vf[d] = tr_vflux_win(g, qw, www, k0, d);
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    const float tt = t.a[j] * ia + 0.0f;
+    const float target = (1.0f - wn) * ro.a[j] + wn * rn.a[j];
+    const float num = qo.a[j] * ro.a[j] + step * (tt - g.rdzw[k] * (vf[j + 1] - vf[j]));
+    out.a[j] = num * (1.0f / target);
+  }
+  st4m(q_out + toff + ii, out, k0, 0, g.L);
+}
+
+__global__ void kv_fct_target(HexGeo g, float step, const float* __restrict__ rho_old,
+                              const float* __restrict__ hv, const float* __restrict__ ww,
+                              float* __restrict__ target, int* flag) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const int ii = c * S + k0;
+  const int n = g.deg[c];
+  const float ia = g.inv_area[c];
+  V4 hd = v4zero();
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float ts = -g.csign[c * g.maxE + s];
+    const float dv = g.dv[e];
+    const V4 h = ld4(hv + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) hd.a[j] = hd.a[j] + ts * h.a[j] * dv * ia;
+  }
+  const Win www = win(ww + c * S, k0, S);
+  const V4 ro = ld4(rho_old + ii);
+  V4 td;
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    td.a[j] = ro.a[j] + step * (hd.a[j] - g.rdzw[k] * (www(j + 1) - www(j)));
+    if (k < L && !(td.a[j] > 0.0f)) bad = true;
+  }
+  if (bad) atomicOr(flag, HEX_FLAG_TARGET);
+  st4m(target + ii, td, k0, 0, g.L);
+}
+
+// low-order upwind vertical flux at interface j = k0 + d (old + 0 scalars)
+__device__ __forceinline__ float fct_fcol_win(float step, const Win& o, const Win& ww, int d) {
+  return step * (pos0(ww(d)) * (o(d - 1) + 0.0f) + neg0(ww(d)) * (o(d) + 0.0f));
+}
+__device__ __forceinline__ float fct_vres_win(const HexGeo& g, float step, const Win& q, const Win& o,
+                                              const Win& ww, int k0, int d) {
+  const float h = step * tr_vflux_win(g, q, ww, k0, d);
+  const int j = k0 + d;
+  if (j <= 0 || j >= g.L) return h;
+  return h - fct_fcol_win(step, o, ww, d);
+}
+
+__global__ void kv_fct_cell1(HexGeo g, float step, const float* __restrict__ q_old,
+                             const float* __restrict__ q_stage, const float* __restrict__ rho_old,
+                             const float* __restrict__ hv, const float* __restrict__ ww,
+                             const float* __restrict__ high_e, const float* __restrict__ target,
+                             float* __restrict__ scale_in, float* __restrict__ scale_out, float* __restrict__ mass_out) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const int ii = c * S + k0;
+  const size_t toff = (size_t)blockIdx.z * g.nC * S;
+  const float* ot = q_old + toff;
+  const float* he = high_e + (size_t)blockIdx.z * g.nE * S;
+  const Win ow = win(ot + c * S, k0, S), qw = win(q_stage + toff + c * S, k0, S), www = win(ww + c * S, k0, S);
+  float mn[4], mx[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    const float o = ow(j) + 0.0f;
+    const float a = (k > 0 ? ow(j - 1) : ow(j)) + 0.0f;
+    const float b = (k + 1 < L ? ow(j + 1) : ow(j)) + 0.0f;
+    mn[j] = fminf(fminf(a, o), b);
+    mx[j] = fmaxf(fmaxf(a, o), b);
+  }
+  const int n = g.deg[c];
+  for (int s = 0; s < n; ++s) {
+    const V4 on = ld4(ot + g.coc[c * g.maxE + s] * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      mn[j] = pymin(mn[j], on.a[j] + 0.0f);
+      mx[j] = pymax(mx[j], on.a[j] + 0.0f);
+    }
+  }
+  const V4 ro = ld4(rho_old + ii), td = ld4(target + ii);
+  float mass[4], s_in[4], s_out[4], vr[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) vr[d] = fct_vres_win(g, step, qw, ow, www, k0, d);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    float m = (ow(j) + 0.0f) * ro.a[j];
+    if (k < L - 1) m = m - fct_fcol_win(step, ow, www, j + 1) * g.rdzw[k];
+    if (k >= 1) m = m + fct_fcol_win(step, ow, www, j) * g.rdzw[k];
+    mass[j] = m;
+    s_in[j] = -g.rdzw[k] * (neg0(vr[j + 1]) - pos0(vr[j]));
+    s_out[j] = -g.rdzw[k] * (pos0(vr[j + 1]) - neg0(vr[j]));
+  }
+  const float ia = g.inv_area[c];
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float ts = -g.csign[c * g.maxE + s];
+    const float dvs = g.dv[e] * step;
+    const V4 vel = ld4(hv + e * S + k0), h = ld4(he + e * S + k0);
+    const V4 o0 = ld4(ot + g.coe[2 * e] * S + k0), o1 = ld4(ot + g.coe[2 * e + 1] * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float upw = dvs * (pos0(vel.a[j]) * (o0.a[j] + 0.0f) + neg0(vel.a[j]) * (o1.a[j] + 0.0f));
+      mass[j] = mass[j] + ts * upw * ia;
+      const float hres = step * h.a[j] - upw;
+      const float sr = -ts * hres;
+      s_out[j] = s_out[j] - pos0(sr) * ia;
+      s_in[j] = s_in[j] - neg0(sr) * ia;
+    }
+  }
+  V4 si, so, ms;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float sf = (mx[j] * td.a[j] - mass[j]) / (s_in[j] + 1.0e-20f);
+    si.a[j] = pymin(1.0f, pos0(sf));
+    sf = (mn[j] * td.a[j] - mass[j]) / (s_out[j] - 1.0e-20f);
+    so.a[j] = pymin(1.0f, pos0(sf));
+    ms.a[j] = mass[j];
+  }
+  st4m(scale_in + toff + ii, si, k0, 0, g.L);
+  st4m(scale_out + toff + ii, so, k0, 0, g.L);
+  st4m(mass_out + toff + ii, ms, k0, 0, g.L);
+}
+
+__global__ void kv_fct_edge(HexGeo g, float step, const float* __restrict__ q_old, const float* __restrict__ hv,
+                            const float* __restrict__ high_e, const float* __restrict__ scale_in,
+                            const float* __restrict__ scale_out, float* __restrict__ hres_lim) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const size_t toff = (size_t)blockIdx.z * g.nC * S;
+  const size_t eoff = (size_t)blockIdx.z * g.nE * S;
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  const V4 vel = ld4(hv + e * S + k0), h = ld4(high_e + eoff + e * S + k0);
+  const V4 o0 = ld4(q_old + toff + i0), o1 = ld4(q_old + toff + i1);
+  const V4 so0 = ld4(scale_out + toff + i0), si1 = ld4(scale_in + toff + i1);
+  const V4 si0 = ld4(scale_in + toff + i0), so1 = ld4(scale_out + toff + i1);
+  const float dvs = g.dv[e] * step;
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float upw = dvs * (pos0(vel.a[j]) * (o0.a[j] + 0.0f) + neg0(vel.a[j]) * (o1.a[j] + 0.0f));
+    const float flux = step * h.a[j] - upw;
+    out.a[j] = pos0(flux) * pymin(so0.a[j], si1.a[j]) + neg0(flux) * pymin(si0.a[j], so1.a[j]);
+  }
+  st4m(hres_lim + eoff + e * S + k0, out, k0, 0, g.L);
+}
+
+__global__ void kv_fct_cell2(HexGeo g, float step, const float* __restrict__ q_old,
+                             const float* __restrict__ q_stage, const float* __restrict__ ww,
+                             const float* __restrict__ scale_in, const float* __restrict__ scale_out,
+                             const float* __restrict__ mass_in, const float* __restrict__ hres_lim,
+                             const float* __restrict__ target, float* __restrict__ q_out) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const int ii = c * S + k0;
+  const size_t toff = (size_t)blockIdx.z * g.nC * S;
+  const float* hl = hres_lim + (size_t)blockIdx.z * g.nE * S;
+  V4 mass = ld4(mass_in + toff + ii);
+  const int n = g.deg[c];
+  const float ia = g.inv_area[c];
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float ts = -g.csign[c * g.maxE + s];
+    const V4 h = ld4(hl + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) mass.a[j] = mass.a[j] + ts * h.a[j] * ia;
+  }
+  const Win ow = win(q_old + toff + c * S, k0, S), qw = win(q_stage + toff + c * S, k0, S);
+  const Win www = win(ww + c * S, k0, S);
+  const Win siw = win(scale_in + toff + c * S, k0, S), sow = win(scale_out + toff + c * S, k0, S);
+  float vl[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const float f = fct_vres_win(g, step, qw, ow, www, k0, d);
+    const int j = k0 + d;
+    vl[d] = (j <= 0 || j >= g.L) ? f
+                                 : pos0(f) * pymin(sow(d - 1), siw(d)) + neg0(f) * pymin(sow(d), siw(d - 1));
+  }
+  const V4 td = ld4(target + ii);
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    const float m = mass.a[j] - g.rdzw[k] * (vl[j + 1] - vl[j]);
+    out.a[j] = pos0(m / td.a[j]);
+  }
+  st4m(q_out + toff + ii, out, k0, 0, g.L);
+}

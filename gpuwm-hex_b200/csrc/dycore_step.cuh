@@ -8,12 +8,21 @@ struct Launcher {
   std::vector<HexProfEvent>* prof = nullptr;  // per-launch CUDA events when profiling
   long long count = 0;
   cudaError_t err = cudaSuccess;
-  int epb() const { return ctx.geo.S >= 256 ? 1 : 256 / ctx.geo.S; }
+  int epb(int tpe) const { return tpe >= 256 ? 1 : 256 / tpe; }
   template <class K, class... A>
   void lp(const char* name, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
+    launch(name, ctx.geo.S, n, nz, smem_per_entity, kernel, args...);
+  }
+  // level-vector form: S/4 threads per entity, four levels each
+  template <class K, class... A>
+  void lpv(const char* name, int n, int nz, K kernel, A... args) {
+    launch(name, ctx.geo.S / 4, n, nz, 0, kernel, args...);
+  }
+  template <class K, class... A>
+  void launch(const char* name, int tpe, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
     if (err != cudaSuccess || n <= 0 || nz <= 0) return;
-    const int e = epb();
-    dim3 block(ctx.geo.S, e), grid((n + e - 1) / e, 1, nz);
+    const int e = epb(tpe);
+    dim3 block(tpe, e), grid((n + e - 1) / e, 1, nz);
     HexProfEvent ev{name, nullptr, nullptr};
     if (prof) {
       cudaEventCreate(&ev.start);
@@ -30,14 +39,29 @@ struct Launcher {
   }
 };
 #define LP(L, n, nz, smem, kernel, ...) (L).lp(#kernel, n, nz, smem, kernel, __VA_ARGS__)
+// Stencil kernel with a level-vector form kv_<name>: the profile name stays k_<name>.
+#define LPS(L, n, nz, name, ...)                                     \
+  do {                                                               \
+    if ((L).ctx.level_vector)                                        \
+      (L).lpv("k_" #name, n, nz, kv_##name, __VA_ARGS__);              \
+    else                                                             \
+      (L).lp("k_" #name, n, nz, 0, k_##name, __VA_ARGS__);             \
+  } while (0)
+#define LPSN(L, label, n, nz, name, ...)                             \
+  do {                                                               \
+    if ((L).ctx.level_vector)                                        \
+      (L).lpv(label, n, nz, kv_##name, __VA_ARGS__);                 \
+    else                                                             \
+      (L).lp(label, n, nz, 0, k_##name, __VA_ARGS__);                \
+  } while (0)
 
 static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexCtx& c = L.ctx;
   const HexGeo& g = c.geo;
   HexWork& w = c.w;
-  LP(L, g.nV, 1, 0, k_diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
-  LP(L, g.nC, 1, 0, k_diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
-  L.lp(recompute_v ? "k_diag_edge_v" : "k_diag_edge", g.nE, 1, 0, k_diag_edge, g, u, (const float*)w.pv_vertex,
+  LPS(L, g.nV, 1, diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
+  LPS(L, g.nC, 1, diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
+  LPSN(L, recompute_v ? "k_diag_edge_v" : "k_diag_edge", g.nE, 1, diag_edge, g, u, (const float*)w.pv_vertex,
        (const float*)w.pv_cell, w.v, w.pv_edge, recompute_v);
 }
 
@@ -88,9 +112,9 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
            (const float*)s_in->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
            w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
     }
-    LP(L, g.nE, 1, 0, k_euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
+    LPS(L, g.nE, 1, euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
          (const float*)w.qtot, (const float*)w.cqu, w.euler_ru);
-    LP(L, g.nC, 1, 0, k_euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
+    LPS(L, g.nC, 1, euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
          (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
          w.tend_rho, w.euler_rw);
 
@@ -104,12 +128,12 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
       }
-      LP(L, g.nC, 1, 0, k_hdiv, g, (const float*)cur->rho_u, w.hdiv);
-      LP(L, g.nE, 1, 0, k_edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
+      LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
+      LPS(L, g.nE, 1, edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
            w.edge_theta, w.edge_w);
-      LP(L, g.nE, 1, 0, k_tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
+      LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
            (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
-      LP(L, g.nC, 1, 0, k_tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
+      LPS(L, g.nC, 1, tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
            (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
            (const float*)w.euler_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage);
@@ -120,14 +144,14 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         const float* old_rt = w.rtpp[(n - 1) & 1];
         float* new_rt = w.rtpp[n & 1];
         if (n == 1) {
-          L.lp("k_ac_edge_first", g.nE, 1, 0, k_ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
+          LPSN(L, "k_ac_edge_first", g.nE, 1, ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
                old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         } else {
           // damping of substep n-1 (new = its output, old = its input), then update n
           const float* prev_new = w.rtpp[(n - 1) & 1];
           const float* prev_old = w.rtpp[(n - 2) & 1];
-          L.lp("k_ac_edge", g.nE, 1, 0, k_ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
+          LPSN(L, "k_ac_edge", g.nE, 1, ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
                prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         }
@@ -140,7 +164,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       }
       {
         const int n = stg.acoustic_steps;
-        L.lp("k_ac_edge_damp", g.nE, 1, 0, k_ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
+        LPSN(L, "k_ac_edge_damp", g.nE, 1, ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
              (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
              (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
       }
@@ -148,10 +172,10 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const float inv_steps = 1.0f / (float)stg.acoustic_steps;
       const float inv_splits = 1.0f / (float)ctx.split_steps;
       const int fm = stg.stage == 3 ? flux_mode : 0;
-      LP(L, g.nE, 1, 0, k_recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
+      LPS(L, g.nE, 1, recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
            (const float*)w.ru_avg, (const float*)s_in->rho_p, (const float*)w.rho_pp, o.rho_u, so.u, w.flux_u,
            fm, inv_steps, inv_splits);
-      LP(L, g.nC, 1, 0, k_recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
+      LPS(L, g.nC, 1, recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
            (const float*)s_in->rtheta_p, (const float*)saved->rho_w, (const float*)w.rho_pp, rtpp_final,
            (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
            inv_splits, w.flag);
@@ -172,19 +196,19 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
       if (si < 2 || !ctx.monotonic) {
         const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
-        LP(L, g.nE, nT, 0, k_tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
-        LP(L, g.nC, nT, 0, k_tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LPS(L, g.nE, nT, tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
+        LPS(L, g.nC, nT, tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)out.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, q_next);
       } else {
-        LP(L, g.nC, 1, 0, k_fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
+        LPS(L, g.nC, 1, fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
              (const float*)w.flux_w, w.target, w.flag);
-        LP(L, g.nE, nT, 0, k_tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
-        LP(L, g.nC, nT, 0, k_fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LPS(L, g.nE, nT, tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
+        LPS(L, g.nC, nT, fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass);
-        LP(L, g.nE, nT, 0, k_fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
+        LPS(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
-        LP(L, g.nC, nT, 0, k_fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
+        LPS(L, g.nC, nT, fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
              (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
              (const float*)w.target, q_next);
       }

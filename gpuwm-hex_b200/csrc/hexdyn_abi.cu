@@ -302,6 +302,12 @@ int build(HexDynHandle* h, const HexDynDesc& d) {
   c.dt = d.dt;
   c.split_steps = d.split_steps;
   c.monotonic = d.monotonic;
+  {
+    // HEXDYN_LEVEL_VECTOR=0 selects the one-level-per-thread stencil kernels
+    // (same results bit for bit; kept for comparison)
+    const char* lv = getenv("HEXDYN_LEVEL_VECTOR");
+    c.level_vector = (lv && lv[0] == '0') ? 0 : 1;
+  }
   const int nC = g.nC, nE = g.nE, nV = g.nV, mE = g.maxE;
 
   // integer connectivity and derived slot data
@@ -398,6 +404,9 @@ int build(HexDynHandle* h, const HexDynDesc& d) {
   const float len = d.len_disp > 0.0f ? d.len_disp : d.nominal_min_dc;
   g.smdiv_base = 2.0f * d.smdiv * len;
   g.moist = d.moist;
+  g.winds_zero = 1;
+  for (int k = 0; k < L; ++k)
+    if (d.u_init[k] != 0.0f || d.v_init[k] != 0.0f) g.winds_zero = 0;
 
   // schedules (hexcore/integration.py:104 RKSchedule.from_mpas, order 3)
   const double dt_dyn = d.dt / d.split_steps;
@@ -812,6 +821,7 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   c.dt = src.dt;
   c.split_steps = src.split_steps;
   c.monotonic = src.monotonic;
+  c.level_vector = src.level_vector;
   c.geo = src.geo;
   for (int i = 0; i < 3; ++i) {
     c.dyn[i] = src.dyn[i];

@@ -6,5 +6,6 @@
 
 namespace hexdyn_strict {
 #include "dycore_kernels.cuh"
+#include "dycore_kernels_vec.cuh"
 #include "dycore_step.cuh"
 }  // namespace hexdyn_strict

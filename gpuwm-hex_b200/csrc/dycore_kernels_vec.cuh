@@ -426,15 +426,18 @@ __global__ void kv_tend_cell(HexGeo g, const float* __restrict__ ru, const float
     }
   }
   if (rk_step > 1) {
+    const V4 tc = ld4(theta_s + c * S + k0);
     for (int s = 0; s < n; ++s) {
       const int e = eoc[s];
       const int e0 = g.coe[2 * e], e1 = g.coe[2 * e + 1];
       const float dvs = cs[s] * g.dv[e];
       const V4 r = ld4(ru + e * S + k0), rs = ld4(ru_s + e * S + k0);
-      const V4 t1 = ld4(theta_s + e1 * S + k0), t0 = ld4(theta_s + e0 * S + k0);
+      const V4 tn = ld4(theta_s + (e0 == c ? e1 : e0) * S + k0);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const float corr = dvs * (rs.a[j] - r.a[j]) * 0.5f * (t1.a[j] + t0.a[j]);
+        // theta_s[e1] + theta_s[e0] with this cell as one operand (IEEE
+        // addition commutes, so the operand order changes no bit)
+        const float corr = dvs * (rs.a[j] - r.a[j]) * 0.5f * (tn.a[j] + tc.a[j]);
         res.a[j] = res.a[j] - corr;
       }
     }
@@ -983,4 +986,346 @@ __global__ void kv_fct_cell2(HexGeo g, float step, const float* __restrict__ q_o
     out.a[j] = pos0(m / td.a[j]);
   }
   st4m(q_out + toff + ii, out, k0, 0, g.L);
+}
+
+// ------------------------------------------------ column-sweep kernels
+// The kernels with a sequential sweep down a column (the tridiagonal
+// coefficients and the acoustic w solve) keep the S/4 threads of a column in
+// G consecutive lanes of one warp (G = 8, 16 or 32: blockDim.x = G, the
+// power of two >= S/4), so their phases synchronise with __syncwarp and a
+// block holds 256/G columns.  Lanes with k0 >= S take part in the
+// synchronisation and the shuffles only.  The sweeps run level by level on
+// the column's first lane, in the order of the one-level form, moving four
+// levels per shared-memory access.
+
+__device__ __forceinline__ V4 lds4(const float* p) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  return V4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ void sts4(float* p, const V4& v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
+}
+
+// Neighbour levels across a thread's chunk: the lane below in the column
+// holds level k0-1 as its a[3], the lane above holds k0+4 as its a[0].  All
+// lanes of the warp take part; a value is used only where the one-level form
+// reads that level, which then lies in a live lane of the same column.
+__device__ __forceinline__ float from_below(float a3) { return __shfl_up_sync(0xffffffffu, a3, 1); }
+__device__ __forceinline__ float from_above(float a0) { return __shfl_down_sync(0xffffffffu, a0, 1); }
+
+// hexcore/acoustic_v841.py:81 compute_vertical_implicit_coefficients_v841.
+#define HEX_VCOEFV_SMEM_ARRAYS 3
+__global__ void kv_vcoef(HexGeo g, float dts2, const float* __restrict__ exner, const float* __restrict__ theta,
+                         const float* __restrict__ rtp, const float* __restrict__ cqw,
+                         const float* __restrict__ qtot, float* __restrict__ cofwr, float* __restrict__ cofwz,
+                         float* __restrict__ coftz, float* __restrict__ cofwt, float* __restrict__ a_tri,
+                         float* __restrict__ alpha_tri, float* __restrict__ gamma_tri, int* flag) {
+  extern __shared__ float sm[];
+  const int S = g.S, L = g.L;
+  const int k0 = threadIdx.x * 4;
+  const int c = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool live = c < g.nC && k0 < S;
+  float* s_a = sm + threadIdx.y * S * HEX_VCOEFV_SMEM_ARRAYS;
+  float* s_b = s_a + S;
+  float* s_c = s_b + S;
+  const int ii = c * S + k0;
+  V4 zz = v4zero(), ex = v4zero(), th = v4zero();
+  V4 wr = v4zero(), wz = v4zero(), tz = v4zero(), wt = v4zero();
+  if (live) {
+    zz = ld4(g.zz + ii);
+    ex = ld4(exner + ii);
+    th = ld4(theta + ii);
+  }
+  const float zzm = from_below(zz.a[3]), exm = from_below(ex.a[3]), thm = from_below(th.a[3]);
+  if (live) {
+    const V4 cq = ld4(cqw + ii), qt = ld4(qtot + ii), rb = ld4(g.rho_base + ii), rtb = ld4(g.rtheta_base + ii);
+    const V4 rp = ld4(rtp + ii), eb = ld4(g.exner_base + ii);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      const float zprev = j == 0 ? zzm : zz.a[j - 1];
+      const float eprev = j == 0 ? exm : ex.a[j - 1];
+      const float tprev = j == 0 ? thm : th.a[j - 1];
+      if (k >= 1 && k < L) {
+        const float izz = g.fzm[k] * zz.a[j] + g.fzp[k] * zprev;
+        wr.a[j] = 0.5f * g.g * izz;
+        wz.a[j] = g.c2 * izz * g.rdzu[k] * cq.a[j] * (g.fzm[k] * ex.a[j] + g.fzp[k] * eprev);
+        tz.a[j] = g.fzm[k] * th.a[j] + g.fzp[k] * tprev;
+      }
+      if (k < L) {
+        wt.a[j] = 0.5f * g.rcv * zz.a[j] * g.g * rb.a[j] / (1.0f + qt.a[j]) * ex.a[j]
+                  / ((rtb.a[j] + rp.a[j]) * eb.a[j]);
+      }
+    }
+  }
+  const float tzm = from_below(tz.a[3]), wtm = from_below(wt.a[3]), tzp = from_above(tz.a[0]);
+  V4 av = v4zero(), bv = v4zero(), cv = v4zero();
+  if (live) {
+    const float* rdzw = g.rdzw;
+    const float* etp = g.etp;
+    const float* ewp = g.ewp;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      float a = 0.0f, b = 0.0f, cc = 0.0f;
+      if (k == 0) b = 1.0f;
+      if (k >= 1 && k < L) {
+        const float zzk = zz.a[j], zzb = j == 0 ? zzm : zz.a[j - 1];
+        const float wz_k = wz.a[j], wr_k = wr.a[j], tz_k = tz.a[j], wt_k = wt.a[j];
+        const float tz_m = j == 0 ? tzm : tz.a[j - 1], wt_m = j == 0 ? wtm : wt.a[j - 1];
+        const float tz_p = j == 3 ? tzp : tz.a[j + 1];
+        a = -wz_k * tz_m * rdzw[k - 1] * zzb + wr_k * rdzw[k - 1] - wt_m * tz_m * rdzw[k - 1];
+        a = a * etp[k - 1] * ewp[k - 1];
+        b = wz_k * tz_k * (etp[k] * rdzw[k] * zzk + etp[k - 1] * rdzw[k - 1] * zzb)
+            - tz_k * (etp[k] * wt_k * rdzw[k] - etp[k - 1] * wt_m * rdzw[k - 1])
+            + wr_k * (etp[k] * rdzw[k] - etp[k - 1] * rdzw[k - 1]);
+        b = b * ewp[k];
+        if (k < L - 1) {
+          cc = -wz_k * tz_p * rdzw[k] * zzk - wr_k * rdzw[k] + wt_k * tz_p * rdzw[k];
+          cc = cc * etp[k] * ewp[k + 1];
+        }
+      }
+      av.a[j] = a;
+      bv.a[j] = b;
+      cv.a[j] = cc;
+    }
+    sts4(s_a + k0, av);
+    sts4(s_b + k0, bv);
+    sts4(s_c + k0, cv);
+  }
+  __syncwarp();
+  if (live && k0 == 0) {
+    // alpha overwrites b and gamma overwrites c; level 0 of both is zero
+    float gam = 0.0f;
+    for (int q = 0; q < L; q += 4) {
+      const V4 a4 = lds4(s_a + q);
+      V4 b4 = lds4(s_b + q), c4 = lds4(s_c + q);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int kk = q + j;
+        if (kk == 0) {
+          b4.a[0] = 0.0f;
+          c4.a[0] = 0.0f;
+        } else if (kk < L) {
+          const float den = 1.0f + dts2 * (b4.a[j] - a4.a[j] * gam);
+          if (den == 0.0f) atomicOr(flag, HEX_FLAG_SINGULAR);
+          const float alpha = 1.0f / den;
+          gam = dts2 * c4.a[j] * alpha;
+          b4.a[j] = alpha;
+          c4.a[j] = gam;
+        }
+      }
+      sts4(s_b + q, b4);
+      sts4(s_c + q, c4);
+    }
+  }
+  __syncwarp();
+  if (live) {
+    st4m(coftz + ii, tz, k0, 0, L + 1);
+    st4m(cofwr + ii, wr, k0, 0, L);
+    st4m(cofwz + ii, wz, k0, 0, L);
+    st4m(cofwt + ii, wt, k0, 0, L);
+    st4m(a_tri + ii, av, k0, 0, L);
+    st4m(alpha_tri + ii, lds4(s_b + k0), k0, 0, L);
+    st4m(gamma_tri + ii, lds4(s_c + k0), k0, 0, L);
+  }
+}
+
+// One acoustic cell pass (hexcore/acoustic_v841.py:461-567): the phases and
+// expressions of k_ac_cell, four levels per thread; only the sweep's
+// operands go through shared memory.
+#define HEX_ACV_SMEM_ARRAYS 4
+__global__ void kv_ac_cell(HexGeo g, int first, float dts, float dts2, const float* __restrict__ ru_p,
+                           const float* __restrict__ theta_s, const float* __restrict__ tend_rho,
+                           const float* __restrict__ tend_rt, const float* __restrict__ tend_rw,
+                           const float* __restrict__ cofwr, const float* __restrict__ cofwz,
+                           const float* __restrict__ coftz, const float* __restrict__ cofwt,
+                           const float* __restrict__ a_tri, const float* __restrict__ alpha_tri,
+                           const float* __restrict__ gamma_tri, const float* __restrict__ rho_zz,
+                           const float* __restrict__ w, const float* __restrict__ rw,
+                           const float* __restrict__ rw_save, const float* __restrict__ rtpp_old,
+                           float* __restrict__ rtpp_new, float* __restrict__ rho_pp, float* __restrict__ rw_p,
+                           float* __restrict__ ww_avg) {
+  extern __shared__ float sm[];
+  const int S = g.S, L = g.L;
+  const int k0 = threadIdx.x * 4;
+  const int c = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool live = c < g.nC && k0 < S;
+  float* s_r = sm + threadIdx.y * S * HEX_ACV_SMEM_ARRAYS;
+  float* s_da = s_r + S;
+  float* s_al = s_da + S;
+  float* s_ga = s_al + S;
+  const int ii = c * S + k0;
+  const float* ewm = g.ewm;
+  const float* ewp = g.ewp;
+  const float* etp = g.etp;
+  const float* etm = g.etm;
+  // phase 1: old rw_p, the edge-flux sums, rs/ts and the ww_avg partial
+  V4 rwp_old = v4zero(), ctz = v4zero(), wa = v4zero();
+  V4 rs = v4zero(), ts = v4zero(), rho_old = v4zero(), rt_old = v4zero();
+  if (live) {
+    if (!first) {
+      const V4 t = ld4rw(rw_p + ii);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rwp_old.a[j] = k0 + j <= L ? t.a[j] : 0.0f;
+    }
+    ctz = ld4(coftz + ii);
+  }
+  const float r4 = from_above(rwp_old.a[0]), ctz4 = from_above(ctz.a[0]);
+  if (live) {
+    const V4 at = ld4(a_tri + ii);
+    V4 da;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) da.a[j] = dts2 * at.a[j];
+    sts4(s_da + k0, da);
+    sts4(s_al + k0, ld4(alpha_tri + ii));
+    sts4(s_ga + k0, ld4(gamma_tri + ii));
+    if (!first) {
+      rho_old = ld4rw(rho_pp + ii);
+      rt_old = ld4(rtpp_old + ii);
+    }
+    const int n = g.deg[c];
+    const float ia = g.inv_area[c];
+    const V4 tc = ld4(theta_s + ii);
+    for (int s = 0; s < n; ++s) {
+      const int e = g.eoc[c * g.maxE + s];
+      const int e0 = g.coe[2 * e], e1 = g.coe[2 * e + 1];
+      const float sdd = g.csign[c * g.maxE + s] * dts * g.dv[e];
+      const V4 r = ld4(ru_p + e * S + k0), tn = ld4(theta_s + (e0 == c ? e1 : e0) * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float flux = sdd * r.a[j] * ia;
+        rs.a[j] = rs.a[j] - flux;
+        // theta_s[e1] + theta_s[e0], one of the two being this cell (IEEE
+        // addition commutes, so the order of the operands changes no bit)
+        ts.a[j] = ts.a[j] - flux * 0.5f * (tn.a[j] + tc.a[j]);
+      }
+    }
+    const V4 trho = ld4(tend_rho + ii), trt = ld4(tend_rt + ii);
+    const V4 wav = first ? v4zero() : ld4rw(ww_avg + ii);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      if (k < L) {
+        const float rnext = j == 3 ? r4 : rwp_old.a[j + 1];
+        const float cnext = j == 3 ? ctz4 : ctz.a[j + 1];
+        const float cofrz = g.rdzw[k];
+        rs.a[j] = rho_old.a[j] + dts * trho.a[j] + rs.a[j]
+                  - dts * cofrz * (ewm[k + 1] * rnext - ewm[k] * rwp_old.a[j]);
+        ts.a[j] = rt_old.a[j] + dts * trt.a[j] + ts.a[j]
+                  - dts * g.rdzw[k] * (ewm[k + 1] * cnext * rnext - ewm[k] * ctz.a[j] * rwp_old.a[j]);
+      }
+      if (k >= 1 && k < L) wa.a[j] = wav.a[j] + ewm[k] * rwp_old.a[j];
+    }
+  }
+  // phase 2: right-hand side of the w system (levels k-1 from the lane below)
+  V4 zz = v4zero(), cwt = v4zero();
+  if (live) {
+    zz = ld4(g.zz + ii);
+    cwt = ld4(cofwt + ii);
+  }
+  const float ts_m = from_below(ts.a[3]), rt_m = from_below(rt_old.a[3]), rs_m = from_below(rs.a[3]);
+  const float rho_m = from_below(rho_old.a[3]), zz_m = from_below(zz.a[3]), cwt_m = from_below(cwt.a[3]);
+  V4 rhs = rwp_old;
+  if (live) {
+    const V4 trw = ld4(tend_rw + ii), cwz = ld4(cofwz + ii), cwr = ld4(cofwr + ii);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      if (k >= 1 && k < L) {
+        const float zzk = zz.a[j], zzm = j == 0 ? zz_m : zz.a[j - 1];
+        const float tsk = ts.a[j], tsm = j == 0 ? ts_m : ts.a[j - 1];
+        const float rtk = rt_old.a[j], rtm = j == 0 ? rt_m : rt_old.a[j - 1];
+        const float rsk = rs.a[j], rsm = j == 0 ? rs_m : rs.a[j - 1];
+        const float rhk = rho_old.a[j], rhm = j == 0 ? rho_m : rho_old.a[j - 1];
+        const float cwtm = j == 0 ? cwt_m : cwt.a[j - 1];
+        rhs.a[j] = rwp_old.a[j] + dts * (trw.a[j]
+                                         - cwz.a[j] * ((etp[k] * zzk * tsk - etp[k - 1] * zzm * tsm)
+                                                       + (etm[k] * zzk * rtk - etm[k - 1] * zzm * rtm))
+                                         - cwr.a[j] * ((etp[k] * rsk + etp[k - 1] * rsm)
+                                                       + (etm[k] * rhk + etm[k - 1] * rhm))
+                                         + cwt.a[j] * (etp[k] * tsk + etm[k] * rtk)
+                                         + cwtm * (etp[k - 1] * tsm + etm[k - 1] * rtm));
+      }
+    }
+    sts4(s_r + k0, rhs);
+  }
+  __syncwarp();
+  // phase 3: the dts^2 Thomas sweep (hexcore/acoustic_v841.py:236-257)
+  if (live && k0 == 0) {
+    float prev = s_r[0];
+    for (int q = 0; q < L; q += 4) {
+      V4 r = lds4(s_r + q);
+      const V4 d = lds4(s_da + q), al = lds4(s_al + q);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int kk = q + j;
+        if (kk >= 1 && kk < L) {
+          prev = (r.a[j] - d.a[j] * prev) * al.a[j];
+          r.a[j] = prev;
+        }
+      }
+      sts4(s_r + q, r);
+    }
+    float next = s_r[L];
+    for (int q = ((L - 1) / 4) * 4; q >= 0; q -= 4) {
+      V4 r = lds4(s_r + q);
+      const V4 ga = lds4(s_ga + q);
+#pragma unroll
+      for (int j = 3; j >= 0; --j) {
+        const int kk = q + j;
+        if (kk < L) {
+          next = r.a[j] - ga.a[j] * next;
+          r.a[j] = next;
+        }
+      }
+      sts4(s_r + q, r);
+    }
+  }
+  __syncwarp();
+  // phase 4: implicit Rayleigh damping, ww_avg, rw_p
+  V4 rwp = v4zero(), rz = v4zero();
+  if (live) {
+    rwp = lds4(s_r + k0);
+    rz = ld4(rho_zz + ii);
+  }
+  const float rz_m = from_below(rz.a[3]);
+  if (live) {
+    const V4 rsv = ld4(rw_save + ii), rwv = ld4(rw + ii), dss = ld4(g.dss + ii), wv = ld4(w + ii);
+    V4 wo;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      wo.a[j] = 0.0f;
+      if (k >= 1 && k < L) {
+        const float delta = rsv.a[j] - rwv.a[j];
+        const float damp = dss.a[j];
+        const float zzi = g.fzm[k] * zz.a[j] + g.fzp[k] * (j == 0 ? zz_m : zz.a[j - 1]);
+        const float rhoi = g.fzm[k] * rz.a[j] + g.fzp[k] * (j == 0 ? rz_m : rz.a[j - 1]);
+        rwp.a[j] = (rwp.a[j] + delta - dts * damp * zzi * rhoi * wv.a[j]) / (1.0f + dts * damp) - delta;
+        wo.a[j] = wa.a[j] + ewp[k] * rwp.a[j];
+      }
+    }
+    st4m(ww_avg + ii, wo, k0, 0, L + 1);
+    st4m(rw_p + ii, rwp, k0, 0, L + 1);
+  }
+  // phase 5: rho_pp and rtheta_pp from the new rw_p (level k+1 from the lane above)
+  const float rwp4 = from_above(rwp.a[0]);
+  if (live) {
+    V4 rpo, rto;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      rpo.a[j] = 0.0f;
+      rto.a[j] = 0.0f;
+      if (k < L) {
+        const float rnext = j == 3 ? rwp4 : rwp.a[j + 1];
+        const float cnext = j == 3 ? ctz4 : ctz.a[j + 1];
+        rpo.a[j] = rs.a[j] - dts * g.rdzw[k] * (ewp[k + 1] * rnext - ewp[k] * rwp.a[j]);
+        rto.a[j] = ts.a[j] - dts * g.rdzw[k] * (ewp[k + 1] * cnext * rnext - ewp[k] * ctz.a[j] * rwp.a[j]);
+      }
+    }
+    st4m(rho_pp + ii, rpo, k0, 0, L);
+    st4m(rtpp_new + ii, rto, k0, 0, L);
+  }
 }

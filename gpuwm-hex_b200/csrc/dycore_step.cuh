@@ -18,6 +18,15 @@ struct Launcher {
   void lpv(const char* name, int n, int nz, K kernel, A... args) {
     launch(name, ctx.geo.S / 4, n, nz, 0, kernel, args...);
   }
+  // column-group form: G lanes of one warp per column (0 when S/4 > 32)
+  int group() const {
+    const int q = ctx.geo.S / 4;
+    return q <= 8 ? 8 : q <= 16 ? 16 : q <= 32 ? 32 : 0;
+  }
+  template <class K, class... A>
+  void lpg(const char* name, int n, size_t smem_per_entity, K kernel, A... args) {
+    launch(name, group(), n, 1, smem_per_entity, kernel, args...);
+  }
   template <class K, class... A>
   void launch(const char* name, int tpe, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
     if (err != cudaSuccess || n <= 0 || nz <= 0) return;
@@ -54,6 +63,15 @@ struct Launcher {
     else                                                             \
       (L).lp(label, n, nz, 0, k_##name, __VA_ARGS__);                \
   } while (0)
+// Column-sweep kernel with a column-group form kv_<name> (shared memory
+// per column: smem for the one-level form, smem_v for the column-group form).
+#define LPG(L, label, n, smem, smem_v, name, ...)                      \
+  do {                                                                 \
+    if ((L).ctx.level_vector && (L).group())                           \
+      (L).lpg(label, n, smem_v, kv_##name, __VA_ARGS__);               \
+    else                                                               \
+      (L).lp(label, n, 1, smem, k_##name, __VA_ARGS__);                \
+  } while (0)
 
 static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexCtx& c = L.ctx;
@@ -89,6 +107,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   HexWork& w = ctx.w;
   const int nT = ctx.n_scalars;
   const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * HEX_AC_SMEM_ARRAYS;
+  const size_t sm_vcoef_v = sizeof(float) * g.S * HEX_VCOEFV_SMEM_ARRAYS;
+  const size_t sm_ac_v = sizeof(float) * g.S * HEX_ACV_SMEM_ARRAYS;
 
   if (g.moist) {
     LP(L, g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
@@ -108,7 +128,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
     const int flux_mode = 4 | (sub == 0 ? 1 : 0) | (last ? 2 : 0);
     // vertical coefficients before RK (stage-1 acoustic dts, saved theta)
     {
-      LP(L, g.nC, 1, sm_vcoef, k_vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
+      LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
            (const float*)s_in->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
            w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
     }
@@ -124,7 +144,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const HexStage& stg = ctx.dyn[si];
       const float dts = (float)stg.acoustic_dt;
       if (stg.stage == 2) {
-        LP(L, g.nC, 1, sm_vcoef, k_vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
+        LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
       }
@@ -155,7 +175,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
                prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         }
-        L.lp(n == 1 ? "k_ac_cell_first" : "k_ac_cell", g.nC, 1, sm_ac, k_ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
+        LPG(L, n == 1 ? "k_ac_cell_first" : "k_ac_cell", g.nC, sm_ac, sm_ac_v, ac_cell, g, n == 1 ? 1 : 0, dts, dts2, (const float*)w.ru_p,
              (const float*)s_in->theta_m, (const float*)w.tend_rho, (const float*)w.tend_rt,
              (const float*)w.tend_rw, (const float*)w.cofwr, (const float*)w.cofwz, (const float*)w.coftz,
              (const float*)w.cofwt, (const float*)w.a_tri, (const float*)w.alpha_tri, (const float*)w.gamma_tri,

@@ -1,16 +1,35 @@
 // Level-vector kernels: each thread owns four consecutive levels of one
 // entity and moves them with 128-bit loads and stores.  The [entity][level]
 // layout with a stride S that is a multiple of 8 makes every 4-level chunk
-// 16-byte aligned.  Per-level arithmetic is exactly the scalar kernels'
-// (the reference's order); only the data movement is vectorised, so the
-// index loads, coefficient loads and address arithmetic of an entity are
-// shared by four levels and each thread carries four independent chains.
+// 16-byte aligned.  Per-level arithmetic follows the reference's expressions
+// and order exactly (one FP32 rounding per operation in the strict build);
+// the index loads, coefficient loads and address arithmetic of an entity
+// are shared by its four levels and each thread carries four independent
+// chains.  Stores are masked to the levels a field defines (levels < L, or
+// <= L for interface fields); padding words are never written.
 //
 // Thread layout: blockDim = (S/4, EPB4); x selects the chunk k0 = 4*x.
+
+// Blocks hold at most 256 threads (S/4 <= 256, checked at create).  The
+// resident-block target per SM sets the register cap: 4 blocks allow 64
+// registers a thread, 3 allow 80.
+#ifndef HEX_VEC_MIN_BLOCKS
+#define HEX_VEC_MIN_BLOCKS 4
+#endif
+#define HEX_VEC_BOUNDS __launch_bounds__(256, HEX_VEC_MIN_BLOCKS)
 
 #define HEX_VEC_PARALLEL(n)                                \
   const int k0 = threadIdx.x * 4;                          \
   const int ent = blockIdx.x * blockDim.y + threadIdx.y;   \
+  if (ent >= (n)) return;
+
+// Transport kernels over nT tracers: block b serves tracer b % nT of entity
+// block b / nT, so the nT tracers of an entity block run back to back and
+// share the reads of the velocities and stencil tables through L2.
+#define HEX_VEC_TRACER(n, nT)                                     \
+  const int k0 = threadIdx.x * 4;                                 \
+  const int tr = blockIdx.x % (nT);                               \
+  const int ent = (blockIdx.x / (nT)) * blockDim.y + threadIdx.y; \
   if (ent >= (n)) return;
 
 struct V4 {
@@ -32,8 +51,7 @@ __device__ __forceinline__ V4 ld4rw(const float* p) {
 __device__ __forceinline__ void st4(float* p, const V4& v) {
   *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
 }
-// Store the lanes whose level k0+j lies in [lo, hi): the levels the
-// one-level-per-thread form of the kernel writes; other words are untouched.
+// Store the lanes whose level k0+j lies in [lo, hi); other words are untouched.
 __device__ __forceinline__ void st4m(float* p, const V4& v, int k0, int lo, int hi) {
   if (k0 >= lo && k0 + 4 <= hi) {
     st4(p, v);
@@ -67,7 +85,7 @@ __device__ __forceinline__ Win win(const float* __restrict__ col, int k0, int S)
 // ---------------------------------------------------------- diagnostics
 // hexcore/diagnostics.py:95 compute_solve_diagnostics, v8.4.1 stored inverses.
 
-__global__ void kv_diag_vertex(HexGeo g, const float* __restrict__ u, float* __restrict__ pv_vertex,
+__global__ void HEX_VEC_BOUNDS kv_diag_vertex(HexGeo g, const float* __restrict__ u, float* __restrict__ pv_vertex,
                                float* __restrict__ ke_vertex) {
   HEX_VEC_PARALLEL(g.nV)
   const int v = ent, S = g.S;
@@ -95,7 +113,8 @@ __global__ void kv_diag_vertex(HexGeo g, const float* __restrict__ u, float* __r
   st4m(ke_vertex + v * S + k0, kv, k0, 0, g.L);
 }
 
-__global__ void kv_diag_cell(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
+// Cell kinetic energy (v8.4.1 kite blend 0.625) and, with APVM, cell PV.
+__global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
                              const float* __restrict__ ke_vertex, float* __restrict__ ke_out,
                              float* __restrict__ pv_cell) {
   HEX_VEC_PARALLEL(g.nC)
@@ -133,7 +152,8 @@ __global__ void kv_diag_cell(HexGeo g, const float* __restrict__ u, const float*
   }
 }
 
-__global__ void kv_diag_edge(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
+// Tangential velocity (TRiSK weights) and edge PV with APVM upwinding.
+__global__ void HEX_VEC_BOUNDS kv_diag_edge(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
                              const float* __restrict__ pv_cell, float* __restrict__ v, float* __restrict__ pv_edge,
                              int recompute_v) {
   HEX_VEC_PARALLEL(g.nE)
@@ -180,7 +200,7 @@ __device__ __forceinline__ float dpdz_of(const HexGeo& g, float rp, float qt, fl
 }
 
 // hexcore/dynamics.py:188 pressure_gradient_euler_tendency.
-__global__ void kv_euler_edge(HexGeo g, const float* __restrict__ pp, const float* __restrict__ rp,
+__global__ void HEX_VEC_BOUNDS kv_euler_edge(HexGeo g, const float* __restrict__ pp, const float* __restrict__ rp,
                               const float* __restrict__ qtot, const float* __restrict__ cqu,
                               float* __restrict__ euler_ru) {
   HEX_VEC_PARALLEL(g.nE)
@@ -222,7 +242,7 @@ __device__ __forceinline__ V4 mass_flux_div4(const HexGeo& g, const float* __res
 }
 
 // hexcore/dynamics.py:122 density_tendency and hexcore/driver.py:2804 Euler w.
-__global__ void kv_euler_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ rw,
+__global__ void HEX_VEC_BOUNDS kv_euler_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ rw,
                               const float* __restrict__ pp, const float* __restrict__ rp,
                               const float* __restrict__ qtot, const float* __restrict__ cqw,
                               float* __restrict__ tend_rho, float* __restrict__ euler_rw) {
@@ -253,15 +273,15 @@ __global__ void kv_euler_cell(HexGeo g, const float* __restrict__ ru, const floa
 }
 
 // ------------------------------------------------- stage tendencies
-
-__global__ void kv_hdiv(HexGeo g, const float* __restrict__ ru, float* __restrict__ hdiv) {
+// hexcore/dynamics.py:86 mass_flux_divergence of the stage rho*u.
+__global__ void HEX_VEC_BOUNDS kv_hdiv(HexGeo g, const float* __restrict__ ru, float* __restrict__ hdiv) {
   HEX_VEC_PARALLEL(g.nC)
   st4m(hdiv + ent * g.S + k0, mass_flux_div4(g, ru, ent, k0), k0, 0, g.L);
 }
 
 // Third-order edge values of theta_m (levels) and w (interfaces):
 // hexcore/driver.py:1023-1034 and :1159-1172.
-__global__ void kv_edge_adv(HexGeo g, const float* __restrict__ ru, const float* __restrict__ theta,
+__global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ ru, const float* __restrict__ theta,
                             const float* __restrict__ w, float* __restrict__ edge_theta,
                             float* __restrict__ edge_w) {
   HEX_VEC_PARALLEL(g.nE)
@@ -308,7 +328,7 @@ __device__ __forceinline__ float wduz_win(const HexGeo& g, const Win& uw, const 
 }
 
 // tend_ru: vertical transport + hexcore/dynamics_v841.py:121 momentum + saved Euler.
-__global__ void kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
+__global__ void HEX_VEC_BOUNDS kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
                           const float* __restrict__ rho, const float* __restrict__ pv_edge,
                           const float* __restrict__ ke, const float* __restrict__ hdiv,
                           const float* __restrict__ euler_ru, float* __restrict__ tend_ru) {
@@ -396,7 +416,7 @@ __device__ __forceinline__ float vflux_w_win(const HexGeo& g, const Win& w, cons
 
 // tend_rt (hexcore/driver.py:933), tend_rw (:1081) + Euler w, then
 // hexcore/acoustic.py:246 convert_w_tendency_to_omega.
-__global__ void kv_tend_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ ru_s,
+__global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ ru_s,
                              const float* __restrict__ rw, const float* __restrict__ rws,
                              const float* __restrict__ theta, const float* __restrict__ theta_s,
                              const float* __restrict__ w, const float* __restrict__ edge_theta,
@@ -495,9 +515,11 @@ __global__ void kv_tend_cell(HexGeo g, const float* __restrict__ ru, const float
 
 // ------------------------------------------------------------- acoustic
 
-// One acoustic edge pass (see k_ac_edge): mode 0 first substep, 1 damping of
-// the previous substep + update, 2 damping only.
-__global__ void kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float damp_coef,
+// One acoustic edge pass: the 3-D divergence damping of the previous
+// substep (hexcore/mixing.py:851, stored inverse of dts), then the ru_p
+// update of this substep (hexcore/acoustic_v841.py:416-460).  mode 0: first
+// substep (ru_p = dts*tend_ru); 1: damping + update; 2: damping only.
+__global__ void HEX_VEC_BOUNDS kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float damp_coef,
                            const float* __restrict__ tend_ru, const float* __restrict__ rtpp_new,
                            const float* __restrict__ rtpp_old, const float* __restrict__ rho_pp,
                            const float* __restrict__ theta_s, const float* __restrict__ exner_s,
@@ -546,8 +568,10 @@ __global__ void kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float
 }
 
 // ---------------------------------------------------------- stage recovery
-
-__global__ void kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, const float* __restrict__ ru_p,
+// hexcore/driver.py:3166-3292 stage recovery, edge part: ru = ru_s + ru_p,
+// u = 2 ru / (rho1 + rho2) (hexcore/driver.py:866), and the split mass-flux
+// average (hexcore/integration.py:27,58).
+__global__ void HEX_VEC_BOUNDS kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, const float* __restrict__ ru_p,
                                 const float* __restrict__ ru_avg, const float* __restrict__ rp_s,
                                 const float* __restrict__ rho_pp, float* __restrict__ ru_out,
                                 float* __restrict__ u_out, float* __restrict__ flux_u, int flux_mode,
@@ -584,7 +608,10 @@ __global__ void kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, const 
   }
 }
 
-__global__ void kv_recover_cell(HexGeo g, int stage3, const float* __restrict__ rp_s,
+// hexcore/driver.py:3166-3292 stage recovery, cell part: candidate state,
+// rw end conditions, theta_m, Exner and p' at stage 3, w from
+// hexcore/terrain.py:491 recover_velocities, and the split w-flux average.
+__global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float* __restrict__ rp_s,
                                 const float* __restrict__ rtp_s, const float* __restrict__ rw_s,
                                 const float* __restrict__ rho_pp, const float* __restrict__ rtpp,
                                 const float* __restrict__ rw_p, const float* __restrict__ ww_avg,
@@ -710,12 +737,14 @@ __global__ void kv_recover_cell(HexGeo g, int stage3, const float* __restrict__ 
 }
 
 // ------------------------------------------------------------ transport
-
-__global__ void kv_tr_edge(HexGeo g, int mono, const float* __restrict__ q, const float* __restrict__ hv,
+// hexcore/transport.py:1461 third-order edge values, one tracer per block
+// row.  mono: the monotonic source flux (velocity folded in; the literal
+// ten-term association for ten-cell stencils).
+__global__ void HEX_VEC_BOUNDS kv_tr_edge(HexGeo g, int nT, int mono, const float* __restrict__ q, const float* __restrict__ hv,
                            float* __restrict__ out) {
-  HEX_VEC_PARALLEL(g.nE)
+  HEX_VEC_TRACER(g.nE, nT)
   const int e = ent, S = g.S;
-  const float* qt = q + (size_t)blockIdx.z * g.nC * S;
+  const float* qt = q + (size_t)tr * g.nC * S;
   const int n = g.n_adv[e];
   const int* cells = g.adv_cells + (size_t)e * g.advW;
   const float* a1 = g.adv + (size_t)e * g.advW;
@@ -753,7 +782,7 @@ __global__ void kv_tr_edge(HexGeo g, int mono, const float* __restrict__ q, cons
       }
     }
   }
-  st4m(out + (size_t)blockIdx.z * g.nE * S + e * S + k0, res, k0, 0, g.L);
+  st4m(out + (size_t)tr * g.nE * S + e * S + k0, res, k0, 0, g.L);
 }
 
 // transport vertical flux at interface j = k0 + d (hexcore/transport.py:1389).
@@ -767,16 +796,17 @@ __device__ __forceinline__ float tr_vflux_win(const HexGeo& g, const Win& q, con
   return base + corr;
 }
 
-__global__ void kv_tr_std(HexGeo g, float step, float wn, const float* __restrict__ q_old,
+// hexcore/transport.py:1649 advance_scalars (RK1/RK2 of split transport).
+__global__ void HEX_VEC_BOUNDS kv_tr_std(HexGeo g, int nT, float step, float wn, const float* __restrict__ q_old,
                           const float* __restrict__ q_stage, const float* __restrict__ rho_old,
                           const float* __restrict__ rho_new, const float* __restrict__ hv,
                           const float* __restrict__ ww, const float* __restrict__ edge_q,
                           float* __restrict__ q_out) {
-  HEX_VEC_PARALLEL(g.nC)
+  HEX_VEC_TRACER(g.nC, nT)
   const int c = ent, S = g.S;
   const int ii = c * S + k0;
-  const size_t toff = (size_t)blockIdx.z * g.nC * S;
-  const float* ev = edge_q + (size_t)blockIdx.z * g.nE * S;
+  const size_t toff = (size_t)tr * g.nC * S;
+  const float* ev = edge_q + (size_t)tr * g.nE * S;
   const int n = g.deg[c];
   V4 t = v4zero();
   for (int s = 0; s < n; ++s) {
@@ -804,7 +834,8 @@ __global__ void kv_tr_std(HexGeo g, float step, float wn, const float* __restric
   st4m(q_out + toff + ii, out, k0, 0, g.L);
 }
 
-__global__ void kv_fct_target(HexGeo g, float step, const float* __restrict__ rho_old,
+// hexcore/transport.py:1887-1906 split-transport target density.
+__global__ void HEX_VEC_BOUNDS kv_fct_target(HexGeo g, float step, const float* __restrict__ rho_old,
                               const float* __restrict__ hv, const float* __restrict__ ww,
                               float* __restrict__ target, int* flag) {
   HEX_VEC_PARALLEL(g.nC)
@@ -847,17 +878,19 @@ __device__ __forceinline__ float fct_vres_win(const HexGeo& g, float step, const
   return h - fct_fcol_win(step, o, ww, d);
 }
 
-__global__ void kv_fct_cell1(HexGeo g, float step, const float* __restrict__ q_old,
+// hexcore/transport.py:1919-2118 (v8.4.1 order): bounds, low-order mass,
+// incoming/outgoing antidiffusive totals and the scale factors.
+__global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const float* __restrict__ q_old,
                              const float* __restrict__ q_stage, const float* __restrict__ rho_old,
                              const float* __restrict__ hv, const float* __restrict__ ww,
                              const float* __restrict__ high_e, const float* __restrict__ target,
                              float* __restrict__ scale_in, float* __restrict__ scale_out, float* __restrict__ mass_out) {
-  HEX_VEC_PARALLEL(g.nC)
+  HEX_VEC_TRACER(g.nC, nT)
   const int c = ent, S = g.S, L = g.L;
   const int ii = c * S + k0;
-  const size_t toff = (size_t)blockIdx.z * g.nC * S;
+  const size_t toff = (size_t)tr * g.nC * S;
   const float* ot = q_old + toff;
-  const float* he = high_e + (size_t)blockIdx.z * g.nE * S;
+  const float* he = high_e + (size_t)tr * g.nE * S;
   const Win ow = win(ot + c * S, k0, S), qw = win(q_stage + toff + c * S, k0, S), www = win(ww + c * S, k0, S);
   float mn[4], mx[4];
 #pragma unroll
@@ -923,13 +956,14 @@ __global__ void kv_fct_cell1(HexGeo g, float step, const float* __restrict__ q_o
   st4m(mass_out + toff + ii, ms, k0, 0, g.L);
 }
 
-__global__ void kv_fct_edge(HexGeo g, float step, const float* __restrict__ q_old, const float* __restrict__ hv,
+// hexcore/transport.py:1919-2118: the limited antidiffusive edge flux.
+__global__ void HEX_VEC_BOUNDS kv_fct_edge(HexGeo g, int nT, float step, const float* __restrict__ q_old, const float* __restrict__ hv,
                             const float* __restrict__ high_e, const float* __restrict__ scale_in,
                             const float* __restrict__ scale_out, float* __restrict__ hres_lim) {
-  HEX_VEC_PARALLEL(g.nE)
+  HEX_VEC_TRACER(g.nE, nT)
   const int e = ent, S = g.S;
-  const size_t toff = (size_t)blockIdx.z * g.nC * S;
-  const size_t eoff = (size_t)blockIdx.z * g.nE * S;
+  const size_t toff = (size_t)tr * g.nC * S;
+  const size_t eoff = (size_t)tr * g.nE * S;
   const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
   const V4 vel = ld4(hv + e * S + k0), h = ld4(high_e + eoff + e * S + k0);
   const V4 o0 = ld4(q_old + toff + i0), o1 = ld4(q_old + toff + i1);
@@ -946,16 +980,17 @@ __global__ void kv_fct_edge(HexGeo g, float step, const float* __restrict__ q_ol
   st4m(hres_lim + eoff + e * S + k0, out, k0, 0, g.L);
 }
 
-__global__ void kv_fct_cell2(HexGeo g, float step, const float* __restrict__ q_old,
+// hexcore/transport.py:1919-2118: limited update of the monotonic stage.
+__global__ void HEX_VEC_BOUNDS kv_fct_cell2(HexGeo g, int nT, float step, const float* __restrict__ q_old,
                              const float* __restrict__ q_stage, const float* __restrict__ ww,
                              const float* __restrict__ scale_in, const float* __restrict__ scale_out,
                              const float* __restrict__ mass_in, const float* __restrict__ hres_lim,
                              const float* __restrict__ target, float* __restrict__ q_out) {
-  HEX_VEC_PARALLEL(g.nC)
+  HEX_VEC_TRACER(g.nC, nT)
   const int c = ent, S = g.S;
   const int ii = c * S + k0;
-  const size_t toff = (size_t)blockIdx.z * g.nC * S;
-  const float* hl = hres_lim + (size_t)blockIdx.z * g.nE * S;
+  const size_t toff = (size_t)tr * g.nC * S;
+  const float* hl = hres_lim + (size_t)tr * g.nE * S;
   V4 mass = ld4(mass_in + toff + ii);
   const int n = g.deg[c];
   const float ia = g.inv_area[c];
@@ -995,8 +1030,8 @@ __global__ void kv_fct_cell2(HexGeo g, float step, const float* __restrict__ q_o
 // power of two >= S/4), so their phases synchronise with __syncwarp and a
 // block holds 256/G columns.  Lanes with k0 >= S take part in the
 // synchronisation and the shuffles only.  The sweeps run level by level on
-// the column's first lane, in the order of the one-level form, moving four
-// levels per shared-memory access.
+// the column's first lane in level order (the order of the one-level forms
+// k_vcoef and k_ac_cell), moving four levels per shared-memory access.
 
 __device__ __forceinline__ V4 lds4(const float* p) {
   const float4 t = *reinterpret_cast<const float4*>(p);
@@ -1015,7 +1050,7 @@ __device__ __forceinline__ float from_above(float a0) { return __shfl_down_sync(
 
 // hexcore/acoustic_v841.py:81 compute_vertical_implicit_coefficients_v841.
 #define HEX_VCOEFV_SMEM_ARRAYS 3
-__global__ void kv_vcoef(HexGeo g, float dts2, const float* __restrict__ exner, const float* __restrict__ theta,
+__global__ void HEX_VEC_BOUNDS kv_vcoef(HexGeo g, float dts2, const float* __restrict__ exner, const float* __restrict__ theta,
                          const float* __restrict__ rtp, const float* __restrict__ cqw,
                          const float* __restrict__ qtot, float* __restrict__ cofwr, float* __restrict__ cofwz,
                          float* __restrict__ coftz, float* __restrict__ cofwt, float* __restrict__ a_tri,
@@ -1135,7 +1170,7 @@ __global__ void kv_vcoef(HexGeo g, float dts2, const float* __restrict__ exner, 
 // expressions of k_ac_cell, four levels per thread; only the sweep's
 // operands go through shared memory.
 #define HEX_ACV_SMEM_ARRAYS 4
-__global__ void kv_ac_cell(HexGeo g, int first, float dts, float dts2, const float* __restrict__ ru_p,
+__global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float dts2, const float* __restrict__ ru_p,
                            const float* __restrict__ theta_s, const float* __restrict__ tend_rho,
                            const float* __restrict__ tend_rt, const float* __restrict__ tend_rw,
                            const float* __restrict__ cofwr, const float* __restrict__ cofwz,

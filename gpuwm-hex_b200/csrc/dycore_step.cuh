@@ -27,11 +27,24 @@ struct Launcher {
   void lpg(const char* name, int n, size_t smem_per_entity, K kernel, A... args) {
     launch(name, group(), n, 1, smem_per_entity, kernel, args...);
   }
+  // level-vector form over nz tracers folded into the block index: block b
+  // serves tracer b % nz (the kernel takes nz as its argument after the
+  // geometry)
+  template <class K, class... A>
+  void lpvt(const char* name, int n, int nz, K kernel, A... args) {
+    launch_impl(name, ctx.geo.S / 4, n, nz, 0, true, kernel, args...);
+  }
   template <class K, class... A>
   void launch(const char* name, int tpe, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
+    launch_impl(name, tpe, n, nz, smem_per_entity, false, kernel, args...);
+  }
+  template <class K, class... A>
+  void launch_impl(const char* name, int tpe, int n, int nz, size_t smem_per_entity, bool fold, K kernel,
+                   A... args) {
     if (err != cudaSuccess || n <= 0 || nz <= 0) return;
     const int e = epb(tpe);
-    dim3 block(tpe, e), grid((n + e - 1) / e, 1, nz);
+    const unsigned nb = (unsigned)((n + e - 1) / e);
+    dim3 block(tpe, e), grid(fold ? nb * (unsigned)nz : nb, 1, fold ? 1 : nz);
     HexProfEvent ev{name, nullptr, nullptr};
     if (prof) {
       cudaEventCreate(&ev.start);
@@ -48,26 +61,17 @@ struct Launcher {
   }
 };
 #define LP(L, n, nz, smem, kernel, ...) (L).lp(#kernel, n, nz, smem, kernel, __VA_ARGS__)
-// Stencil kernel with a level-vector form kv_<name>: the profile name stays k_<name>.
-#define LPS(L, n, nz, name, ...)                                     \
-  do {                                                               \
-    if ((L).ctx.level_vector)                                        \
-      (L).lpv("k_" #name, n, nz, kv_##name, __VA_ARGS__);              \
-    else                                                             \
-      (L).lp("k_" #name, n, nz, 0, k_##name, __VA_ARGS__);             \
-  } while (0)
-#define LPSN(L, label, n, nz, name, ...)                             \
-  do {                                                               \
-    if ((L).ctx.level_vector)                                        \
-      (L).lpv(label, n, nz, kv_##name, __VA_ARGS__);                 \
-    else                                                             \
-      (L).lp(label, n, nz, 0, k_##name, __VA_ARGS__);                \
-  } while (0)
-// Column-sweep kernel with a column-group form kv_<name> (shared memory
-// per column: smem for the one-level form, smem_v for the column-group form).
+// Stencil kernel kv_<name> (four levels per thread), profiled as k_<name>.
+#define LPS(L, n, nz, name, ...) (L).lpv("k_" #name, n, nz, kv_##name, __VA_ARGS__)
+#define LPSN(L, label, n, nz, name, ...) (L).lpv(label, n, nz, kv_##name, __VA_ARGS__)
+// Transport kernel kv_<name> over nT tracers (tracer folded into the block index).
+#define LPST(L, n, nT, name, g, ...) (L).lpvt("k_" #name, n, nT, kv_##name, g, nT, __VA_ARGS__)
+// Column-sweep kernel: the column-group form kv_<name> when a column fits in
+// one warp (S/4 <= 32), else the one-level form k_<name> (shared memory per
+// column: smem_v and smem respectively).
 #define LPG(L, label, n, smem, smem_v, name, ...)                      \
   do {                                                                 \
-    if ((L).ctx.level_vector && (L).group())                           \
+    if ((L).group())                                                   \
       (L).lpg(label, n, smem_v, kv_##name, __VA_ARGS__);               \
     else                                                               \
       (L).lp(label, n, 1, smem, k_##name, __VA_ARGS__);                \
@@ -216,19 +220,19 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
       if (si < 2 || !ctx.monotonic) {
         const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
-        LPS(L, g.nE, nT, tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
-        LPS(L, g.nC, nT, tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LPST(L, g.nE, nT, tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
+        LPST(L, g.nC, nT, tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)out.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, q_next);
       } else {
         LPS(L, g.nC, 1, fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
              (const float*)w.flux_w, w.target, w.flag);
-        LPS(L, g.nE, nT, tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
-        LPS(L, g.nC, nT, fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
+        LPST(L, g.nE, nT, tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
+        LPST(L, g.nC, nT, fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass);
-        LPS(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
+        LPST(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
-        LPS(L, g.nC, nT, fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
+        LPST(L, g.nC, nT, fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
              (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
              (const float*)w.target, q_next);
       }

@@ -219,6 +219,9 @@ int validate(const HexDynDesc* d) {
     return fail(HEXDYN_E_ARG, "mesh sizes must be positive");
   if (d->n_levels < 4)
     return fail(HEXDYN_E_ARG, "n_levels=%d: the third-order vertical fluxes need at least 4 levels", d->n_levels);
+  if (d->n_levels > 1000)
+    return fail(HEXDYN_E_ARG, "n_levels=%d: at most 1000 levels (a column's four-level chunks fill one block)",
+                d->n_levels);
   if (d->max_edges <= 0 || d->max_edges2 <= 0 || d->adv_width <= 0 || d->n_scalars < 0)
     return fail(HEXDYN_E_ARG, "invalid slot widths or scalar count");
   if (d->max_edges > 8 || d->max_edges2 > 16 || d->adv_width > 16)
@@ -302,12 +305,6 @@ int build(HexDynHandle* h, const HexDynDesc& d) {
   c.dt = d.dt;
   c.split_steps = d.split_steps;
   c.monotonic = d.monotonic;
-  {
-    // HEXDYN_LEVEL_VECTOR=0 selects the one-level-per-thread stencil kernels
-    // (same results bit for bit; kept for comparison)
-    const char* lv = getenv("HEXDYN_LEVEL_VECTOR");
-    c.level_vector = (lv && lv[0] == '0') ? 0 : 1;
-  }
   const int nC = g.nC, nE = g.nE, nV = g.nV, mE = g.maxE;
 
   // integer connectivity and derived slot data
@@ -821,7 +818,6 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   c.dt = src.dt;
   c.split_steps = src.split_steps;
   c.monotonic = src.monotonic;
-  c.level_vector = src.level_vector;
   c.geo = src.geo;
   for (int i = 0; i < 3; ++i) {
     c.dyn[i] = src.dyn[i];

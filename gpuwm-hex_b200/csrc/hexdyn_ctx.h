@@ -78,7 +78,6 @@ struct HexCtx {
   int parity = 0;       // 0: state in `in`, 1: state in `out`
   long long steps_done = 0;
   long long launches_per_step = 0;
-  int level_vector = 1;  // 1: stencil kernels take four levels per thread
 };
 
 namespace hexdyn_strict {

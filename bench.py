@@ -52,6 +52,10 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
+    ap.add_argument("--batched", default="on", choices=["on", "off"],
+                    help="also time the uneven ensemble (24 x 10242-cell members at 1440 s + 16 x 40962-cell "
+                         "members at 720 s) batched and looped")
+    ap.add_argument("--batch-periods", type=int, default=4, help="timed 1440 s periods of the ensemble leg")
     return ap.parse_args()
 
 
@@ -206,6 +210,115 @@ def cores_used() -> int:
     return 1
 
 
+# ------------------------------------------------------------- ensembles
+ENSEMBLE = ((5, 24, 1440.0, 1), (6, 16, 720.0, 2))  # (level, members, dt, steps per 1440 s period)
+
+
+def build_ensemble(args, plain_case):
+    """The uneven ensemble: per mesh, members that share its geometry and
+    differ in a seeded theta perturbation (0.1 K, smoothed over 3 rings) and
+    tracer blobs; qv plus 2 condensates."""
+    from hexdyn.case import build_case
+    from hexdyn.mesh import build_mesh
+
+    groups = []
+    for gi, (level, n, dt, per) in enumerate(ENSEMBLE):
+        mesh = plain_case.mesh if level == args.level else build_mesh(level, lloyd=20, seed=0)
+        base = plain_case if level == args.level else build_case(mesh, n_levels=args.levels, seed=0,
+                                                                   n_condensates=2)
+        members = [build_case(mesh, n_levels=args.levels, seed=1000 * (gi + 1) + i, n_condensates=2,
+                              theta_noise=0.1, theta_noise_rings=3, like=base) for i in range(n)]
+        groups.append((members, dt, per))
+    return groups
+
+
+def run_ensemble(args, stream, dist, world: int, rank: int, plain_case) -> dict:
+    """Member-days per hour of the uneven ensemble, batched (one ensemble
+    handle per time step, both advanced by hexdyn_step_batched: every kernel
+    launch covers all members of a group, the groups run concurrently) and
+    looped (each member its own single-instance graph, one after another).
+    Members are spread over ranks by cell count (no per-step collective)."""
+    import torch
+
+    import hexdyn
+    from hexdyn.config import DycoreConfig
+    from hexdyn.ensemble import HexEnsemble, assign_members, step_batched
+
+    groups = build_ensemble(args, plain_case)
+    flat = [(gi, m) for gi, (members, _, _) in enumerate(groups) for m in range(len(members))]
+    cells = [groups[gi][0][m].mesh.n_cells for gi, m in flat]
+    mine = set(assign_members(cells, world)[rank])
+    cfgs = [DycoreConfig(config_dt=dt, config_number_of_sub_steps=2, moist_coefficients="native",
+                         numerics=args.numerics) for _, dt, _ in groups]
+    my_groups = []
+    for gi, (members, dt, per) in enumerate(groups):
+        sel = [members[m] for i, (g, m) in enumerate(flat) if g == gi and i in mine]
+        my_groups.append((sel, per))
+    n_members = sum(len(sel) for sel, _ in my_groups)
+    periods, warm = max(1, args.batch_periods), 2
+
+    def timed(run):
+        for _ in range(warm):
+            run()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(periods):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # looped: every member its own single-instance driver (whole step as a graph)
+    singles = [(hexdyn.from_case(c, cfgs[gi], capture_graph=True), per)
+               for gi, (sel, per) in enumerate(my_groups) for c in sel]
+
+    def looped():
+        for drv, per in singles:
+            drv.step_async(per)
+
+    loop_ms = timed(looped)
+    loop_flags = [drv.read_flag() for drv, _ in singles]
+    launches_single = sum(drv.receipt().launches_per_step * per for drv, per in singles)
+    for drv, _ in singles:
+        drv.close()
+    del singles
+    # batched: one ensemble per time step, both groups per call
+    ens = [(HexEnsemble.from_cases(sel, cfgs[gi], capture_graph=True), per)
+           for gi, (sel, per) in enumerate(my_groups) if sel]
+
+    def batched():
+        step_batched([e for e, _ in ens], [per for _, per in ens], read_flags=False, stream=stream)
+
+    batch_ms = timed(batched)
+    batch_flags = [e.read_flag() for e, _ in ens]
+    launches_batched = sum(e.receipt().launches_per_step * per for e, per in ens)
+    for e, _ in ens:
+        e.close()
+    total_members = len(flat)
+    period_days = 1440.0 / 86400.0
+    batched_value = total_members * periods * period_days / (batch_ms / 1000.0 / 3600.0)
+    looped_value = total_members * periods * period_days / (loop_ms / 1000.0 / 3600.0)
+    return {
+        "metric": "member-days/hour", "value": batched_value, "looped_value": looped_value,
+        "speedup_vs_looped": batched_value / looped_value,
+        "ms_per_period": batch_ms / periods, "looped_ms_per_period": loop_ms / periods,
+        "periods": periods, "warmup": warm, "members": total_members, "members_this_rank": n_members,
+        "workload": "uneven ensemble: 24 members on the 10242-cell mesh (dt 1440 s, 1 step per period) + 16 "
+                    "members on the 40962-cell mesh (dt 720 s, 2 steps per period), 55 levels, qv + 2 "
+                    "condensates, theta noise 0.1 K over 3 rings; a period is 1440 simulated seconds",
+        "gpu_launches_per_period": int(launches_batched), "looped_gpu_launches_per_period": int(launches_single),
+        "validation_flags": [*loop_flags, *batch_flags],
+    }
+
+
 # ------------------------------------------------------------------- arms
 def run_reference(args, rank: int) -> None:
     if rank != 0:
@@ -347,6 +460,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     e2e_value = world * (e2e_steps * dt / 86400.0) / (e2e_ms / 1000.0 / 3600.0)
     drv.read_flag()
 
+    batched = run_ensemble(args, stream, dist, world, rank, case) if args.batched == "on" else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, n = oracle_time_per_step(case, dt, args.cpu_budget_s, 2)
@@ -374,6 +489,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "step_bytes_algorithmic": step_bytes,
             "step_gbs": step_bytes / (ms_per_step / 1000.0) / 1e9,
             "kernels": kernels,
+            "batched": batched,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

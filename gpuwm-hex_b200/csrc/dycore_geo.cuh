@@ -73,6 +73,7 @@ struct HexGeo {
   float kappa;        // FP32(R/(cp-R)) computed in double then rounded
   float apvm_scale;   // FP32(apvm)*FP32(dt)
   float smdiv_base;   // 2*smdiv*len_disp in FP32 operations
+  const float* smdiv_edge;  // [E] smdiv_base of the edge's mesh (ensembles mix meshes)
   int apvm_on;
   int moist;          // 0 = dry coefficients, 1 = native (all scalars load)
   int winds_zero;     // u_init and v_init are zero at every level

@@ -519,7 +519,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
 // substep (hexcore/mixing.py:851, stored inverse of dts), then the ru_p
 // update of this substep (hexcore/acoustic_v841.py:416-460).  mode 0: first
 // substep (ru_p = dts*tend_ru); 1: damping + update; 2: damping only.
-__global__ void HEX_VEC_BOUNDS kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float damp_coef,
+__global__ void HEX_VEC_BOUNDS kv_ac_edge(HexGeo g, int mode, int old_is_zero, float dts, float inv_dts,
                            const float* __restrict__ tend_ru, const float* __restrict__ rtpp_new,
                            const float* __restrict__ rtpp_old, const float* __restrict__ rho_pp,
                            const float* __restrict__ theta_s, const float* __restrict__ exner_s,
@@ -537,6 +537,8 @@ __global__ void HEX_VEC_BOUNDS kv_ac_edge(HexGeo g, int mode, int old_is_zero, f
     return;
   }
   const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  // smdiv_base * (1/dts), the damping coefficient of the edge's mesh
+  const float damp_coef = g.smdiv_edge[e] * inv_dts;
   V4 r = ld4rw(ru_p + jj);
   const V4 n0 = ld4(rtpp_new + i0), n1 = ld4(rtpp_new + i1);
   const V4 o0 = old_is_zero ? v4zero() : ld4(rtpp_old + i0);

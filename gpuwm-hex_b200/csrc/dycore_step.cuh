@@ -162,20 +162,20 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
            (const float*)w.euler_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage);
       // acoustic substeps
-      const float damp = g.smdiv_base * (1.0f / dts);
+      const float inv_dts = 1.0f / dts;
       const float dts2 = stg.dts2;
       for (int n = 1; n <= stg.acoustic_steps; ++n) {
         const float* old_rt = w.rtpp[(n - 1) & 1];
         float* new_rt = w.rtpp[n & 1];
         if (n == 1) {
-          LPSN(L, "k_ac_edge_first", g.nE, 1, ac_edge, g, 0, 1, dts, damp, (const float*)w.tend_ru, (const float*)new_rt,
+          LPSN(L, "k_ac_edge_first", g.nE, 1, ac_edge, g, 0, 1, dts, inv_dts, (const float*)w.tend_ru, (const float*)new_rt,
                old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         } else {
           // damping of substep n-1 (new = its output, old = its input), then update n
           const float* prev_new = w.rtpp[(n - 1) & 1];
           const float* prev_old = w.rtpp[(n - 2) & 1];
-          LPSN(L, "k_ac_edge", g.nE, 1, ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru, prev_new,
+          LPSN(L, "k_ac_edge", g.nE, 1, ac_edge, g, 1, n - 1 == 1 ? 1 : 0, dts, inv_dts, (const float*)w.tend_ru, prev_new,
                prev_old, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
         }
@@ -188,7 +188,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       }
       {
         const int n = stg.acoustic_steps;
-        LPSN(L, "k_ac_edge_damp", g.nE, 1, ac_edge, g, 2, n == 1 ? 1 : 0, dts, damp, (const float*)w.tend_ru,
+        LPSN(L, "k_ac_edge_damp", g.nE, 1, ac_edge, g, 2, n == 1 ? 1 : 0, dts, inv_dts, (const float*)w.tend_ru,
              (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
              (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
       }

@@ -21,6 +21,14 @@ struct HexDynHandle {
   size_t staging_count[HEXDYN_NUM_FIELDS] = {};
   int* host_flag = nullptr;
   bool have_state[HEXDYN_NUM_FIELDS] = {};
+  // ensemble members: first cell / edge / vertex and counts of each member in
+  // the concatenated mesh (one member for a single instance), and the fields
+  // each member has been given
+  std::vector<int> m_c0, m_e0, m_v0, m_nc, m_ne, m_nv;
+  std::vector<unsigned> m_have;
+  // private stream and events of hexdyn_step_batched
+  cudaStream_t batch_stream = nullptr;
+  cudaEvent_t batch_fork = nullptr, batch_done = nullptr;
 };
 
 namespace {
@@ -287,7 +295,9 @@ int validate(const HexDynDesc* d) {
   return HEXDYN_OK;
 }
 
-int build(HexDynHandle* h, const HexDynDesc& d) {
+// smdiv_edge: per-edge 2*smdiv*len_disp for ensembles of several meshes;
+// NULL gives every edge the descriptor's value.
+int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_edge = nullptr) {
   HexCtx& c = h->ctx;
   HexGeo& g = c.geo;
   const int L = d.n_levels;
@@ -400,6 +410,10 @@ int build(HexDynHandle* h, const HexDynDesc& d) {
   g.apvm_scale = d.apvm_upwinding * (float)d.dt;
   const float len = d.len_disp > 0.0f ? d.len_disp : d.nominal_min_dc;
   g.smdiv_base = 2.0f * d.smdiv * len;
+  {
+    const std::vector<float> sm = smdiv_edge ? *smdiv_edge : std::vector<float>((size_t)nE, g.smdiv_base);
+    if ((e = upload(c, &g.smdiv_edge, sm)) != cudaSuccess) return cuda_fail(e, "upload smdiv_edge");
+  }
   g.moist = d.moist;
   g.winds_zero = 1;
   for (int k = 0; k < L; ++k)
@@ -493,6 +507,13 @@ int hexdyn_create(const HexDynDesc* desc, HexDynHandle** out) {
     hexdyn_destroy(h);
     return rc;
   }
+  h->m_c0 = {0};
+  h->m_e0 = {0};
+  h->m_v0 = {0};
+  h->m_nc = {desc->n_cells};
+  h->m_ne = {desc->n_edges};
+  h->m_nv = {desc->n_vertices};
+  h->m_have = {0u};
   *out = h;
   return HEXDYN_OK;
 }
@@ -689,7 +710,339 @@ int hexdyn_destroy(HexDynHandle* h) {
   }
   for (void* p : c.allocations) cudaFree(p);
   if (h->host_flag) cudaFreeHost(h->host_flag);
+  if (h->batch_fork) cudaEventDestroy(h->batch_fork);
+  if (h->batch_done) cudaEventDestroy(h->batch_done);
+  if (h->batch_stream) cudaStreamDestroy(h->batch_stream);
   delete h;
+  return HEXDYN_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ ensembles
+// An ensemble handle holds several members as one mesh: member m's cells,
+// edges and vertices are a contiguous range of the concatenated mesh, its
+// connectivity is offset into that range, and no stencil reaches across
+// members.  Every kernel of the step therefore computes each member exactly
+// as a handle of its own would, in one launch for all members.
+
+namespace {
+
+template <class T>
+bool same_bits(const T* a, const T* b, size_t n) {
+  return memcmp(a, b, n * sizeof(T)) == 0;
+}
+
+// Owns the arrays of the concatenated descriptor.
+struct MergedDesc {
+  HexDynDesc d{};
+  std::vector<int32_t> coe, eoc, coc, voc, deg, voe, eov, cov, eoe, neoe, advc, nadv;
+  std::vector<float> dc, dv, area, area_tri, kite, weights, fv, fe, cosa, sina, adv, adv3;
+  std::vector<float> zz, zxu, dss, zb, zb3, rb, rtb, eb;
+  std::vector<float> smdiv_edge;
+};
+
+int check_compatible(const HexDynDesc& a, const HexDynDesc& b, int m) {
+  const int L = a.n_levels;
+  auto bad = [&](const char* what) {
+    return fail(HEXDYN_E_ARG, "ensemble member %d differs from member 0 in %s (members of one ensemble share "
+                "the configuration, levels, tracers and vertical coordinate)", m, what);
+  };
+  if (b.n_levels != L) return bad("n_levels");
+  if (b.n_scalars != a.n_scalars) return bad("n_scalars");
+  if (b.dt != a.dt) return bad("dt");
+  if (b.n_sub_steps != a.n_sub_steps || b.split_steps != a.split_steps) return bad("the schedule");
+  if (b.monotonic != a.monotonic || b.moist != a.moist || b.numerics != a.numerics) return bad("the options");
+  const float fa[] = {a.coef_3rd_order, a.apvm_upwinding, a.smdiv, a.len_disp, a.epssm_minimum, a.epssm_maximum,
+                      a.epssm_bottom_z, a.epssm_top_z, a.rgas, a.cp, a.gravity, a.p0, a.cf1, a.cf2, a.cf3,
+                      a.acoustic_dts2[0], a.acoustic_dts2[1], a.acoustic_dts2[2]};
+  const float fb[] = {b.coef_3rd_order, b.apvm_upwinding, b.smdiv, b.len_disp, b.epssm_minimum, b.epssm_maximum,
+                      b.epssm_bottom_z, b.epssm_top_z, b.rgas, b.cp, b.gravity, b.p0, b.cf1, b.cf2, b.cf3,
+                      b.acoustic_dts2[0], b.acoustic_dts2[1], b.acoustic_dts2[2]};
+  if (!same_bits(fa, fb, sizeof fa / sizeof fa[0])) return bad("a configuration constant");
+  if (!same_bits(a.fzm, b.fzm, L) || !same_bits(a.fzp, b.fzp, L) || !same_bits(a.rdzw, b.rdzw, L) ||
+      !same_bits(a.rdzu, b.rdzu, L))
+    return bad("the vertical coordinate");
+  if (!same_bits(a.u_init, b.u_init, L) || !same_bits(a.v_init, b.v_init, L)) return bad("the reference winds");
+  return HEXDYN_OK;
+}
+
+// [rows][n_m] blocks of every member -> [rows][sum n]
+void cat_rows(std::vector<float>& out, const HexDynDesc* ds, int n, int rows, const float* HexDynDesc::*field,
+              const std::vector<int>& off, const std::vector<int>& cnt, size_t total) {
+  out.assign((size_t)rows * total, 0.0f);
+  for (int m = 0; m < n; ++m)
+    for (int r = 0; r < rows; ++r)
+      memcpy(&out[(size_t)r * total + off[m]], ds[m].*field + (size_t)r * cnt[m], cnt[m] * sizeof(float));
+}
+
+// [n_m][w_m] rows of every member -> [sum n][w], entries + shift (ints)
+void cat_slots(std::vector<int32_t>& out, const HexDynDesc* ds, int n, const int32_t* const HexDynDesc::*field,
+               const std::vector<int>& cnt, const std::vector<int>& wm, int w, const std::vector<int>& shift,
+               size_t total) {
+  out.assign(total * w, 0);
+  size_t row = 0;
+  for (int m = 0; m < n; ++m)
+    for (int i = 0; i < cnt[m]; ++i, ++row)
+      for (int s = 0; s < wm[m]; ++s) out[row * w + s] = (ds[m].*field)[(size_t)i * wm[m] + s] + shift[m];
+}
+
+void cat_slots_f(std::vector<float>& out, const HexDynDesc* ds, int n, const float* HexDynDesc::*field,
+                 const std::vector<int>& cnt, const std::vector<int>& wm, int w, size_t total) {
+  out.assign(total * w, 0.0f);
+  size_t row = 0;
+  for (int m = 0; m < n; ++m)
+    for (int i = 0; i < cnt[m]; ++i, ++row)
+      for (int s = 0; s < wm[m]; ++s) out[row * w + s] = (ds[m].*field)[(size_t)i * wm[m] + s];
+}
+
+int merge_members(const HexDynDesc* ds, int n, MergedDesc& M, HexDynHandle* h) {
+  const HexDynDesc& a = ds[0];
+  const int L = a.n_levels;
+  std::vector<int> nc(n), ne(n), nv(n), c0(n), e0(n), v0(n), wE(n), wE2(n), wA(n), w3(n, 3), w2(n, 2), w1(n, 1);
+  size_t C = 0, E = 0, V = 0;
+  int mE = 0, mE2 = 0, mA = 0;
+  for (int m = 0; m < n; ++m) {
+    nc[m] = ds[m].n_cells;
+    ne[m] = ds[m].n_edges;
+    nv[m] = ds[m].n_vertices;
+    c0[m] = (int)C;
+    e0[m] = (int)E;
+    v0[m] = (int)V;
+    C += nc[m];
+    E += ne[m];
+    V += nv[m];
+    wE[m] = ds[m].max_edges;
+    wE2[m] = ds[m].max_edges2;
+    wA[m] = ds[m].adv_width;
+    mE = std::max(mE, wE[m]);
+    mE2 = std::max(mE2, wE2[m]);
+    mA = std::max(mA, wA[m]);
+  }
+  if (C > (size_t)INT32_MAX / 64 || E > (size_t)INT32_MAX / 64)
+    return fail(HEXDYN_E_CAPACITY, "ensemble of %zu cells / %zu edges exceeds the int32 index range", C, E);
+  std::vector<int> zero(n, 0);
+  cat_slots(M.coe, ds, n, &HexDynDesc::cells_on_edge, ne, w2, 2, c0, E);
+  cat_slots(M.eoc, ds, n, &HexDynDesc::edges_on_cell, nc, wE, mE, e0, C);
+  cat_slots(M.coc, ds, n, &HexDynDesc::cells_on_cell, nc, wE, mE, c0, C);
+  cat_slots(M.voc, ds, n, &HexDynDesc::vertices_on_cell, nc, wE, mE, v0, C);
+  cat_slots(M.deg, ds, n, &HexDynDesc::n_edges_on_cell, nc, w1, 1, zero, C);
+  cat_slots(M.voe, ds, n, &HexDynDesc::vertices_on_edge, ne, w2, 2, v0, E);
+  cat_slots(M.eov, ds, n, &HexDynDesc::edges_on_vertex, nv, w3, 3, e0, V);
+  cat_slots(M.cov, ds, n, &HexDynDesc::cells_on_vertex, nv, w3, 3, c0, V);
+  cat_slots(M.eoe, ds, n, &HexDynDesc::edges_on_edge, ne, wE2, mE2, e0, E);
+  cat_slots(M.neoe, ds, n, &HexDynDesc::n_edges_on_edge, ne, w1, 1, zero, E);
+  cat_slots(M.advc, ds, n, &HexDynDesc::adv_cells, ne, wA, mA, c0, E);
+  cat_slots(M.nadv, ds, n, &HexDynDesc::n_adv_cells, ne, w1, 1, zero, E);
+  cat_slots_f(M.dc, ds, n, &HexDynDesc::dc_edge, ne, w1, 1, E);
+  cat_slots_f(M.dv, ds, n, &HexDynDesc::dv_edge, ne, w1, 1, E);
+  cat_slots_f(M.area, ds, n, &HexDynDesc::area_cell, nc, w1, 1, C);
+  cat_slots_f(M.area_tri, ds, n, &HexDynDesc::area_triangle, nv, w1, 1, V);
+  cat_slots_f(M.kite, ds, n, &HexDynDesc::kite_areas, nv, w3, 3, V);
+  cat_slots_f(M.weights, ds, n, &HexDynDesc::weights_on_edge, ne, wE2, mE2, E);
+  cat_slots_f(M.fv, ds, n, &HexDynDesc::f_vertex, nv, w1, 1, V);
+  cat_slots_f(M.fe, ds, n, &HexDynDesc::f_edge, ne, w1, 1, E);
+  cat_slots_f(M.cosa, ds, n, &HexDynDesc::cos_angle_edge, ne, w1, 1, E);
+  cat_slots_f(M.sina, ds, n, &HexDynDesc::sin_angle_edge, ne, w1, 1, E);
+  cat_slots_f(M.adv, ds, n, &HexDynDesc::adv_coefs, ne, wA, mA, E);
+  cat_slots_f(M.adv3, ds, n, &HexDynDesc::adv_coefs_3rd, ne, wA, mA, E);
+  cat_rows(M.zz, ds, n, L, &HexDynDesc::zz, c0, nc, C);
+  cat_rows(M.zxu, ds, n, L, &HexDynDesc::zxu, e0, ne, E);
+  cat_rows(M.dss, ds, n, L, &HexDynDesc::dss, c0, nc, C);
+  cat_rows(M.rb, ds, n, L, &HexDynDesc::rho_base, c0, nc, C);
+  cat_rows(M.rtb, ds, n, L, &HexDynDesc::rho_theta_base, c0, nc, C);
+  cat_rows(M.eb, ds, n, L, &HexDynDesc::exner_base, c0, nc, C);
+  // terrain metrics [L+1][C][maxEdges]
+  M.zb.assign((size_t)(L + 1) * C * mE, 0.0f);
+  M.zb3.assign((size_t)(L + 1) * C * mE, 0.0f);
+  for (int m = 0; m < n; ++m)
+    for (int k = 0; k <= L; ++k)
+      for (int i = 0; i < nc[m]; ++i)
+        for (int sl = 0; sl < wE[m]; ++sl) {
+          const size_t src = ((size_t)k * nc[m] + i) * wE[m] + sl, dst = ((size_t)k * C + c0[m] + i) * mE + sl;
+          M.zb[dst] = ds[m].zb_cell[src];
+          M.zb3[dst] = ds[m].zb3_cell[src];
+        }
+  // divergence damping length of each member's mesh (hexcore/mixing.py:851)
+  M.smdiv_edge.assign(E, 0.0f);
+  for (int m = 0; m < n; ++m) {
+    const float len = ds[m].len_disp > 0.0f ? ds[m].len_disp : ds[m].nominal_min_dc;
+    const float base = 2.0f * ds[m].smdiv * len;
+    std::fill(M.smdiv_edge.begin() + e0[m], M.smdiv_edge.begin() + e0[m] + ne[m], base);
+  }
+  HexDynDesc& d = M.d;
+  d = a;
+  d.n_cells = (int)C;
+  d.n_edges = (int)E;
+  d.n_vertices = (int)V;
+  d.max_edges = mE;
+  d.max_edges2 = mE2;
+  d.adv_width = mA;
+  d.cells_on_edge = M.coe.data();
+  d.edges_on_cell = M.eoc.data();
+  d.cells_on_cell = M.coc.data();
+  d.vertices_on_cell = M.voc.data();
+  d.n_edges_on_cell = M.deg.data();
+  d.vertices_on_edge = M.voe.data();
+  d.edges_on_vertex = M.eov.data();
+  d.cells_on_vertex = M.cov.data();
+  d.edges_on_edge = M.eoe.data();
+  d.n_edges_on_edge = M.neoe.data();
+  d.adv_cells = M.advc.data();
+  d.n_adv_cells = M.nadv.data();
+  d.dc_edge = M.dc.data();
+  d.dv_edge = M.dv.data();
+  d.area_cell = M.area.data();
+  d.area_triangle = M.area_tri.data();
+  d.kite_areas = M.kite.data();
+  d.weights_on_edge = M.weights.data();
+  d.f_vertex = M.fv.data();
+  d.f_edge = M.fe.data();
+  d.cos_angle_edge = M.cosa.data();
+  d.sin_angle_edge = M.sina.data();
+  d.adv_coefs = M.adv.data();
+  d.adv_coefs_3rd = M.adv3.data();
+  d.zz = M.zz.data();
+  d.zxu = M.zxu.data();
+  d.dss = M.dss.data();
+  d.zb_cell = M.zb.data();
+  d.zb3_cell = M.zb3.data();
+  d.rho_base = M.rb.data();
+  d.rho_theta_base = M.rtb.data();
+  d.exner_base = M.eb.data();
+  h->m_c0 = c0;
+  h->m_e0 = e0;
+  h->m_v0 = v0;
+  h->m_nc = nc;
+  h->m_ne = ne;
+  h->m_nv = nv;
+  h->m_have.assign(n, 0u);
+  return HEXDYN_OK;
+}
+
+// Member m's slice of a field: entity offset and count.
+void member_slice(const HexDynHandle* h, int field, int m, int* off, int* cnt) {
+  const bool edge = field == HEXDYN_RHO_U || field == HEXDYN_U;
+  *off = edge ? h->m_e0[m] : h->m_c0[m];
+  *cnt = edge ? h->m_ne[m] : h->m_nc[m];
+}
+
+int member_io(HexDynHandle* h, int member, int field, float* host, size_t count, void* stream, bool upload) {
+  if (!h || !host) return fail(HEXDYN_E_ARG, "NULL handle or host pointer");
+  if (field < 0 || field >= HEXDYN_NUM_FIELDS) return fail(HEXDYN_E_ARG, "unknown field %d", field);
+  if (member < 0 || member >= (int)h->m_c0.size())
+    return fail(HEXDYN_E_ARG, "member %d out of range (%zu members)", member, h->m_c0.size());
+  const FieldShape fs = field_shape(h->ctx, field);
+  int off = 0, n = 0;
+  member_slice(h, field, member, &off, &n);
+  const size_t want = (size_t)fs.blocks * fs.rows * n;
+  if (count != want) return fail(HEXDYN_E_ARG, "member %d field %d has %zu values, got %zu", member, field, want, count);
+  if (count == 0) return HEXDYN_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int S = h->ctx.geo.S;
+  float* base = field_ptr(cur_state(h), cur_side(h), field);
+  float* stage = h->staging[field];
+  if (upload) HEX_CUDA(cudaMemcpyAsync(stage, host, count * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+  for (int b = 0; b < fs.blocks; ++b) {
+    dim3 grid((n + 31) / 32, (fs.rows + 31) / 32), block(32, 8);
+    float* dev = base + ((size_t)b * fs.n + off) * S;
+    float* sb = stage + (size_t)b * fs.rows * n;
+    if (upload)
+      k_to_padded<<<grid, block, 0, st>>>(sb, fs.rows, n, S, dev);
+    else
+      k_from_padded<<<grid, block, 0, st>>>(dev, fs.rows, n, S, sb);
+  }
+  HEX_CUDA(cudaGetLastError(), "member transpose");
+  if (!upload) {
+    HEX_CUDA(cudaMemcpyAsync(host, stage, count * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+    return HEXDYN_OK;
+  }
+  h->m_have[member] |= 1u << field;
+  bool all = true;
+  for (unsigned bits : h->m_have) all = all && (bits >> field & 1u);
+  if (all) h->have_state[field] = true;
+  return HEXDYN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hexdyn_create_ensemble(const HexDynDesc* members, int n_members, HexDynHandle** out) {
+  if (!out) return fail(HEXDYN_E_ARG, "out is NULL");
+  *out = nullptr;
+  if (!members || n_members < 1) return fail(HEXDYN_E_ARG, "an ensemble needs at least one member");
+  for (int m = 0; m < n_members; ++m) {
+    int rc = validate(&members[m]);
+    if (rc) return fail(rc, "ensemble member %d: %s", m, g_last_error.c_str());
+    if (m > 0 && (rc = check_compatible(members[0], members[m], m))) return rc;
+  }
+  HexDynHandle* h = new HexDynHandle();
+  MergedDesc M;
+  int rc = merge_members(members, n_members, M, h);
+  if (!rc) rc = validate(&M.d);
+  if (!rc) rc = build(h, M.d, &M.smdiv_edge);
+  if (rc) {
+    hexdyn_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HEXDYN_OK;
+}
+
+int hexdyn_member_count(HexDynHandle* h) { return h ? (int)h->m_c0.size() : 0; }
+
+int hexdyn_set_member_state(HexDynHandle* h, int member, int field, const float* host, size_t count, void* stream) {
+  return member_io(h, member, field, const_cast<float*>(host), count, stream, true);
+}
+
+int hexdyn_get_member_state(HexDynHandle* h, int member, int field, float* host, size_t count, void* stream) {
+  return member_io(h, member, field, host, count, stream, false);
+}
+
+int hexdyn_step_batched(const HexDynBatch* batch, void* stream) {
+  if (!batch || batch->n_groups < 1 || !batch->groups || !batch->steps)
+    return fail(HEXDYN_E_ARG, "batch needs n_groups >= 1, groups and steps");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = batch->n_groups;
+  for (int i = 0; i < n; ++i) {
+    HexDynHandle* h = batch->groups[i];
+    if (!h) return fail(HEXDYN_E_ARG, "batch group %d is NULL", i);
+    if (batch->steps[i] < 0) return fail(HEXDYN_E_ARG, "batch group %d: negative step count", i);
+    for (int j = 0; j < i; ++j)
+      if (batch->groups[j] == h) return fail(HEXDYN_E_ARG, "batch groups %d and %d are the same handle", j, i);
+    if (!h->batch_stream) {
+      HEX_CUDA(cudaStreamCreateWithFlags(&h->batch_stream, cudaStreamNonBlocking), "batch stream");
+      HEX_CUDA(cudaEventCreateWithFlags(&h->batch_fork, cudaEventDisableTiming), "batch event");
+      HEX_CUDA(cudaEventCreateWithFlags(&h->batch_done, cudaEventDisableTiming), "batch event");
+    }
+  }
+  // fork: every group waits for the caller's stream, then steps on its own
+  // stream so that the groups run concurrently; join back into the caller's
+  // stream
+  for (int i = 0; i < n; ++i) {
+    HexDynHandle* h = batch->groups[i];
+    HEX_CUDA(cudaEventRecord(h->batch_fork, st), "fork record");
+    HEX_CUDA(cudaStreamWaitEvent(h->batch_stream, h->batch_fork, 0), "fork wait");
+    int rc = hexdyn_step_async(h, h->batch_stream, batch->steps[i]);
+    if (rc) return fail(rc, "batch group %d: %s", i, g_last_error.c_str());
+    HEX_CUDA(cudaEventRecord(h->batch_done, h->batch_stream), "join record");
+    HEX_CUDA(cudaStreamWaitEvent(st, h->batch_done, 0), "join wait");
+  }
+  if (!batch->flags) return HEXDYN_OK;
+  int bad = -1;
+  for (int i = 0; i < n; ++i) {
+    int f = 0;
+    int rc = hexdyn_read_flag(batch->groups[i], st, &f);
+    batch->flags[i] = f;
+    if (rc == HEXDYN_E_NUMERIC) {
+      if (bad < 0) bad = i;
+    } else if (rc) {
+      return rc;
+    }
+  }
+  if (bad >= 0)
+    return fail(HEXDYN_E_NUMERIC, "batch group %d: device validation flag 0x%x set", bad, batch->flags[bad]);
   return HEXDYN_OK;
 }
 

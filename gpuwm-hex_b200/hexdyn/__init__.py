@@ -6,16 +6,20 @@ CUDA kernels; PyTorch is used only for device tensors and streams.
 
 from .config import ConfigurationRefusal, DycoreConfig
 from .driver import DeviceStepResult, HexDycoreDriver, HostSidecar, HostState, HostStepResult
+from .ensemble import HexEnsemble, assign_members, step_batched
 
 __all__ = [
     "ConfigurationRefusal",
     "DycoreConfig",
     "DeviceStepResult",
     "HexDycoreDriver",
+    "HexEnsemble",
     "HostSidecar",
     "HostState",
     "HostStepResult",
+    "assign_members",
     "from_case",
+    "step_batched",
 ]
 
 

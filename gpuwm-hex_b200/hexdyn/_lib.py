@@ -62,6 +62,13 @@ class HexDynDesc(C.Structure):
     ]
 
 
+class HexDynBatch(C.Structure):
+    """Groups of an uneven batch and their step counts (hexdyn_step_batched)."""
+
+    _fields_ = [("n_groups", C.c_int32), ("groups", C.POINTER(C.c_void_p)),
+                ("steps", C.POINTER(C.c_int32)), ("flags", C.POINTER(C.c_int32))]
+
+
 EXPORTS = {
     "hexdyn_abi_version": (C.c_int, []),
     "hexdyn_create": (C.c_int, [C.POINTER(HexDynDesc), C.POINTER(C.c_void_p)]),
@@ -79,6 +86,11 @@ EXPORTS = {
     "hexdyn_device_bytes": (C.c_size_t, [C.c_void_p]),
     "hexdyn_step_noalloc": (C.c_int, [C.c_void_p, C.POINTER(HexDynFields), C.POINTER(HexDynFields),
                                       C.c_void_p, C.POINTER(C.c_int)]),
+    "hexdyn_create_ensemble": (C.c_int, [C.POINTER(HexDynDesc), C.c_int, C.POINTER(C.c_void_p)]),
+    "hexdyn_member_count": (C.c_int, [C.c_void_p]),
+    "hexdyn_set_member_state": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F32P, C.c_size_t, C.c_void_p]),
+    "hexdyn_get_member_state": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F32P, C.c_size_t, C.c_void_p]),
+    "hexdyn_step_batched": (C.c_int, [C.POINTER(HexDynBatch), C.c_void_p]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -435,15 +435,28 @@ def build_case(mesh: VoronoiMesh, *, n_levels: int = 55, ztop: float = 30000.0,
                seed: int = 0, n_condensates: int = 0, jet_speed: float = 35.0,
                perturbation: float = 1.0, coef_3rd_order: float = 0.25,
                theta_noise: float = 0.0, theta_noise_rings: int = 3,
-               terrain: bool = True) -> DycoreCase:
-    """The balanced-jet dry state with qv (+ condensates) on ``mesh``."""
+               terrain: bool = True, like: DycoreCase | None = None) -> DycoreCase:
+    """The balanced-jet dry state with qv (+ condensates) on ``mesh``.
+
+    ``like``: an earlier case on the same mesh whose terrain, vertical grid,
+    terrain metrics and advection stencil are reused (ensemble members that
+    differ only in their state); ``seed`` then draws only the state's noise
+    and tracer blobs."""
     rng = np.random.default_rng(seed + 1)
     radius = mesh.sphere_radius
-    ter = gaussian_terrain(mesh, seed=seed) if terrain else np.zeros(mesh.n_cells)
-    vertical = build_vertical_grid(mesh, ter, n_levels=n_levels, ztop=ztop)
-    d2 = deriv_two(mesh)
-    zb_cell, zb3_cell = terrain_metrics(mesh, vertical, d2, coef_3rd_order)
-    adv, adv3, n_adv, adv_cells = advection_stencil(mesh, d2)
+    if like is not None:
+        if like.mesh is not mesh or like.vertical.zz.shape[0] != n_levels or like.coef_3rd_order != coef_3rd_order:
+            raise ValueError("like= must be a case on the same mesh, levels and coef_3rd_order")
+        vertical = like.vertical
+        zb_cell, zb3_cell = like.zb_cell, like.zb3_cell
+        adv, adv3, n_adv, adv_cells = (like.adv_coefs, like.adv_coefs_3rd, like.n_adv_cells_for_edge,
+                                       like.adv_cells_for_edge)
+    else:
+        ter = gaussian_terrain(mesh, seed=seed) if terrain else np.zeros(mesh.n_cells)
+        vertical = build_vertical_grid(mesh, ter, n_levels=n_levels, ztop=ztop)
+        d2 = deriv_two(mesh)
+        zb_cell, zb3_cell = terrain_metrics(mesh, vertical, d2, coef_3rd_order)
+        adv, adv3, n_adv, adv_cells = advection_stencil(mesh, d2)
 
     theta0 = 300.0
     lat_g, z_g, theta_g, exner_g = _balanced_jet(jet_speed, 10000.0, theta0, radius)

@@ -17,6 +17,10 @@
  *                              :4854 _step_device_v841 (flag read :5355-5402)
  *   hexdyn_capture_graph    <- hexcore/cuda_subcycle_graphs.py:64 attach_subcycle_graphs
  *                              (here the whole large step is one graph)
+ *   hexdyn_create_ensemble,
+ *   hexdyn_set/get_member_state,
+ *   hexdyn_step_batched     <- hexcore/multi_member.py (members on private
+ *                              streams); batched stepping of uneven ensembles
  *   hexdyn_last_error       <- the refusal / FloatingPointError text of the driver
  *   hexdyn_destroy          <- driver teardown
  *
@@ -197,6 +201,41 @@ typedef struct HexDynFields {
  * hexdyn_step (synchronises `stream`). */
 int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, const HexDynFields* out, void* stream,
                         int* flag_out);
+
+/* Ensembles (hexcore/multi_member.py:1-7 runs members on private streams,
+ * one launch sequence each).  hexdyn_create_ensemble concatenates several
+ * members into one handle: member m keeps its own mesh (meshes may differ in
+ * size), terrain, reference state and state, all members share the
+ * configuration, levels, tracer count and vertical coordinate (refused with
+ * HEXDYN_E_ARG otherwise), and every kernel of the step runs once for all
+ * members.  No stencil crosses members, so each member's result equals, bit
+ * for bit, the step of a handle created from its descriptor alone.  The
+ * whole-field calls (hexdyn_set_state, hexdyn_get_state, hexdyn_step,
+ * hexdyn_capture_graph, ...) act on the concatenation; the member calls move
+ * one member's field in its own logical layout ([level][entity] of that
+ * member). */
+int hexdyn_create_ensemble(const HexDynDesc* members, int n_members, HexDynHandle** out);
+int hexdyn_member_count(HexDynHandle* h);
+int hexdyn_set_member_state(HexDynHandle* h, int member, int field, const float* host, size_t count,
+                            void* stream);
+int hexdyn_get_member_state(HexDynHandle* h, int member, int field, float* host, size_t count, void* stream);
+
+/* Groups of an uneven batch: handles (single instances or ensembles) whose
+ * members differ in time step, each advanced by its own number of large
+ * steps per call (for instance 1 step of 1440 s and 2 steps of 720 s). */
+typedef struct HexDynBatch {
+  int32_t n_groups;
+  HexDynHandle* const* groups;   /* distinct handles */
+  const int32_t* steps;          /* large steps of each group */
+  int32_t* flags;                /* out: validation flag of each group; NULL = do not read */
+} HexDynBatch;
+
+/* Advance every group of the batch, each on the handle's private stream
+ * after the work already on `stream`, and make `stream` wait for all of them
+ * (the groups run concurrently).  With flags != NULL the flags are read and
+ * cleared (synchronises `stream`) and a set flag returns HEXDYN_E_NUMERIC
+ * naming the first group; with flags == NULL nothing synchronises. */
+int hexdyn_step_batched(const HexDynBatch* batch, void* stream);
 
 /* Copy the last error message of this thread into buf. */
 int hexdyn_last_error(char* buf, size_t len);

@@ -56,6 +56,8 @@ def parse() -> argparse.Namespace:
                     help="also time the uneven ensemble (24 x 10242-cell members at 1440 s + 16 x 40962-cell "
                          "members at 720 s) batched and looped")
     ap.add_argument("--batch-periods", type=int, default=4, help="timed 1440 s periods of the ensemble leg")
+    ap.add_argument("--learned", default="on", choices=["on", "off"],
+                    help="also train the learned corrector (shortened) and time the corrected path for half a day")
     return ap.parse_args()
 
 
@@ -319,6 +321,29 @@ def run_ensemble(args, stream, dist, world: int, rank: int, plain_case) -> dict:
     }
 
 
+# ------------------------------------------------------ learned corrector
+def run_learned(args, plain_case) -> dict:
+    """The learned-corrector path on this mesh (qv + 2 condensates, dt 720 s):
+    pairs from 4 members, 30 epochs per network, then half a simulated day
+    of the plain, reduced-with-checks and learned paths from a held-out
+    member.  The 5-day evaluation is ``python -m hexdyn.learned_eval``."""
+    from hexdyn.learned_eval import run
+
+    res = run(level=args.level, levels=args.levels, members=4, epochs=30, days=0.5, mesh=plain_case.mesh)
+    lp = res["learned"]
+    return {
+        "metric": "simulated days/hour", "value": lp["days_per_hour"], "plain_value": res["plain"]["days_per_hour"],
+        "speedup_vs_plain": lp["speedup_vs_plain"], "fallbacks": lp["fallbacks"], "steps": lp["steps_done"],
+        "ps_rms_hpa_vs_plain": lp["ps_rms_hpa"], "theta_rel_l2_vs_plain": lp["theta_rel_l2"],
+        "no_network_value": res["reduced_with_checks_no_network"]["days_per_hour"],
+        "no_network_fallbacks": res["reduced_with_checks_no_network"]["fallbacks"],
+        "reduced_uncorrected_first_flagged_step": res["reduced_uncorrected"]["first_flagged_step"],
+        "column_net_val_loss": res["column_net"]["val_loss"],
+        "column_net_val_loss_no_correction": res["column_net"]["val_loss_no_correction"],
+        "workload": res["workload"] + f"; {res['eval_steps']} steps ({res['eval_days']:g} days)",
+    }
+
+
 # ------------------------------------------------------------------- arms
 def run_reference(args, rank: int) -> None:
     if rank != 0:
@@ -461,6 +486,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     drv.read_flag()
 
     batched = run_ensemble(args, stream, dist, world, rank, case) if args.batched == "on" else None
+    learned = run_learned(args, case) if args.learned == "on" and args.level == 6 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -490,6 +516,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "step_gbs": step_bytes / (ms_per_step / 1000.0) / 1e9,
             "kernels": kernels,
             "batched": batched,
+            "learned": learned,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -1048,6 +1048,183 @@ int hexdyn_step_batched(const HexDynBatch* batch, void* stream) {
 
 }  // extern "C"
 
+// ------------------------------------------------------ learned corrector
+// State access of the learned corrector (no counterpart in the reference):
+// raw input features of the column and edge networks, the application of
+// their output increments to the prognostic state, and the total energy
+// that decides whether a corrected step is accepted.
+
+namespace {
+
+// Column features [C][6L]: theta_m, rho_zz, w (interfaces 0..L-1), the first
+// scalar (qv), the mean of u over the cell's edges, and the mean of theta_m
+// over the neighbouring cells, each for levels 0..L-1.
+__global__ void k_col_features(HexGeo g, HexState s, HexSide d, float* __restrict__ X, int ld) {
+  const int c = blockIdx.x, L = g.L, S = g.S;
+  const int n = g.deg[c];
+  float* row = X + (size_t)c * ld;
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const int i = c * S + k;
+    float um = 0.0f, tm = 0.0f;
+    for (int q = 0; q < n; ++q) {
+      um += d.u[g.eoc[c * g.maxE + q] * S + k];
+      tm += d.theta_m[g.coc[c * g.maxE + q] * S + k];
+    }
+    row[k] = d.theta_m[i];
+    row[L + k] = s.rho[i];
+    row[2 * L + k] = d.w[i];
+    row[3 * L + k] = s.scalars ? s.scalars[i] : 0.0f;
+    row[4 * L + k] = um / (float)n;
+    row[5 * L + k] = tm / (float)n;
+  }
+}
+
+// Edge features [E][4L]: u, theta_m of both cells, mean rho_zz of both cells.
+__global__ void k_edge_features(HexGeo g, HexState s, HexSide d, float* __restrict__ X, int ld) {
+  const int e = blockIdx.x, L = g.L, S = g.S;
+  const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+  float* row = X + (size_t)e * ld;
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    row[k] = d.u[e * S + k];
+    row[L + k] = d.theta_m[c0 * S + k];
+    row[2 * L + k] = d.theta_m[c1 * S + k];
+    row[3 * L + k] = 0.5f * (s.rho[c0 * S + k] + s.rho[c1 * S + k]);
+  }
+}
+
+// Column increments (denormalised y * scale + shift of theta_m, rho_zz, w)
+// applied to the prognostic state: rho' = rho + drho, rho_theta' = rho' *
+// (theta_m + dtheta), rho_w' = rho_w + dw * zz_k * rho'_k at the interfaces
+// 1..L-1 (the interface weights of w recovery).
+__global__ void k_apply_col(HexGeo g, HexState s, HexSide d, const float* __restrict__ Y, int ld,
+                            const float* __restrict__ scale, const float* __restrict__ shift) {
+  const int c = blockIdx.x, L = g.L, S = g.S;
+  const float* y = Y + (size_t)c * ld;
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const int i = c * S + k;
+    const float dth = y[k] * scale[k] + shift[k];
+    const float drho = y[L + k] * scale[L + k] + shift[L + k];
+    const float rho = s.rho[i] + drho;
+    s.rho[i] = rho;
+    s.rho_theta[i] = rho * (d.theta_m[i] + dth);
+  }
+  __syncthreads();
+  for (int k = 1 + threadIdx.x; k < L; k += blockDim.x) {
+    const int i = c * S + k;
+    const float dw = y[2 * L + k] * scale[2 * L + k] + shift[2 * L + k];
+    const float zzi = g.fzm[k] * g.zz[i] + g.fzp[k] * g.zz[i - 1];
+    const float rhoi = g.fzm[k] * s.rho[i] + g.fzp[k] * s.rho[i - 1];
+    s.rho_w[i] = s.rho_w[i] + dw * zzi * rhoi;
+  }
+}
+
+// Edge increments of u: rho_u' = rho_u + du * (rho_zz at the edge).
+__global__ void k_apply_edge(HexGeo g, HexState s, const float* __restrict__ Y, int ld,
+                             const float* __restrict__ scale, const float* __restrict__ shift) {
+  const int e = blockIdx.x, L = g.L, S = g.S;
+  const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+  const float* y = Y + (size_t)e * ld;
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const float du = y[k] * scale[k] + shift[k];
+    s.rho_u[e * S + k] += du * 0.5f * (s.rho[c0 * S + k] + s.rho[c1 * S + k]);
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+  if (threadIdx.x < 32)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Total energy: sum over cells and levels of the mass rho_zz * area * dzw
+// times (cv T + g z) with T = theta_m * exner, plus the vertical kinetic
+// energy rho_w * w / 2 * area / rdzu at the interior interfaces, plus sum
+// over edges and levels of rho_u * u * (dc dv / 2) * dzw / 2.
+__global__ void k_energy(HexGeo g, HexState s, HexSide d, const float* __restrict__ z, float cv,
+                         double* __restrict__ out) {
+  const int L = g.L, S = g.S;
+  double acc = 0.0, w2 = 0.0;
+  const size_t nc = (size_t)g.nC * L, ne = (size_t)g.nE * L;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nc + ne; t += (size_t)gridDim.x * blockDim.x) {
+    if (t < nc) {
+      const int c = (int)(t / L), k = (int)(t % L);
+      const int i = c * S + k;
+      const double mass = (double)s.rho[i] / ((double)g.inv_area[c] * (double)g.rdzw[k]);
+      acc += mass * ((double)cv * d.theta_m[i] * d.exner[i] + (double)g.g * z[i]);
+      if (k >= 1) {
+        const double vol = 1.0 / ((double)g.inv_area[c] * (double)g.rdzu[k]);
+        acc += 0.5 * (double)s.rho_w[i] * d.w[i] * vol;
+        w2 += (double)d.w[i] * d.w[i] * vol;
+      }
+    } else {
+      const size_t te = t - nc;
+      const int e = (int)(te / L), k = (int)(te % L);
+      const int j = e * S + k;
+      acc += 0.25 * (double)s.rho_u[j] * d.u[j] * g.dc[e] * g.dv[e] / (double)g.rdzw[k];
+    }
+  }
+  acc = block_sum(acc);
+  __syncthreads();
+  w2 = block_sum(w2);
+  if (threadIdx.x == 0) {
+    atomicAdd(out, acc);
+    atomicAdd(out + 1, w2);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hexdyn_column_features(HexDynHandle* h, float* X, int ld, void* stream) {
+  if (!h || !X || ld < 6 * h->ctx.geo.L) return fail(HEXDYN_E_ARG, "column features need ld >= 6 L");
+  k_col_features<<<h->ctx.geo.nC, 64, 0, (cudaStream_t)stream>>>(h->ctx.geo, cur_state(h), cur_side(h), X, ld);
+  HEX_CUDA(cudaGetLastError(), "column features");
+  return HEXDYN_OK;
+}
+
+int hexdyn_edge_features(HexDynHandle* h, float* X, int ld, void* stream) {
+  if (!h || !X || ld < 4 * h->ctx.geo.L) return fail(HEXDYN_E_ARG, "edge features need ld >= 4 L");
+  k_edge_features<<<h->ctx.geo.nE, 64, 0, (cudaStream_t)stream>>>(h->ctx.geo, cur_state(h), cur_side(h), X, ld);
+  HEX_CUDA(cudaGetLastError(), "edge features");
+  return HEXDYN_OK;
+}
+
+int hexdyn_apply_increments(HexDynHandle* h, const float* Ycol, int ldc, const float* col_scale,
+                            const float* col_shift, const float* Yedge, int lde, const float* edge_scale,
+                            const float* edge_shift, void* stream) {
+  if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
+  const HexGeo& g = h->ctx.geo;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (Ycol) {
+    if (ldc < 3 * g.L || !col_scale || !col_shift) return fail(HEXDYN_E_ARG, "column increments need ld >= 3 L");
+    k_apply_col<<<g.nC, 64, 0, st>>>(g, cur_state(h), cur_side(h), Ycol, ldc, col_scale, col_shift);
+  }
+  if (Yedge) {
+    if (lde < g.L || !edge_scale || !edge_shift) return fail(HEXDYN_E_ARG, "edge increments need ld >= L");
+    k_apply_edge<<<g.nE, 64, 0, st>>>(g, cur_state(h), Yedge, lde, edge_scale, edge_shift);
+  }
+  HEX_CUDA(cudaGetLastError(), "apply increments");
+  return HEXDYN_OK;
+}
+
+int hexdyn_total_energy(HexDynHandle* h, const float* z_mid, double* dev_out, void* stream) {
+  if (!h || !z_mid || !dev_out) return fail(HEXDYN_E_ARG, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  HEX_CUDA(cudaMemsetAsync(dev_out, 0, 2 * sizeof(double), st), "energy clear");
+  const float cv = h->ctx.geo.c2 / h->ctx.geo.rcv - h->ctx.geo.rgas;
+  k_energy<<<4 * 148, 256, 0, st>>>(h->ctx.geo, cur_state(h), cur_side(h), z_mid, cv, dev_out);
+  HEX_CUDA(cudaGetLastError(), "energy");
+  return HEXDYN_OK;
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------ no-alloc step
 // hexdyn_step_noalloc: the large step with its scratch in a file-scope device
 // array instead of the handle's workspace (declaration and contract in

@@ -1,0 +1,417 @@
+// BF16 tensor-core MLP kernels for the learned corrector: one GEMM kernel on
+// the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor
+// memory) with fused epilogues, and the elementwise kernels of training
+// (loss gradient, bias gradient, Adam).  Declarations: include/hexmlp.h.
+//
+// GEMM: C[M][N] = A[M][K] . B[N][K]^T with A and B bf16, both K-contiguous
+// ("K-major"), FP32 accumulation.  Every product of the network is cast in
+// this form by keeping transposed copies where needed (W^T for the input
+// gradient, H^T and dZ^T for the weight gradient), so one kernel serves the
+// forward pass and both backward products.
+//
+// Tiling: a CTA of 128 threads owns a 128 x BN output tile (BN = 128 or
+// 256) whose FP32 accumulator lives in BN columns of tensor memory (128
+// lanes = 128 rows).  K advances in 64-element slabs through two shared
+// memory stages; the threads fill a stage with 16-byte loads in the
+// canonical K-major no-swizzle layout (8-row x 16-byte core matrices; the
+// descriptor's leading offset steps along K, the stride offset along rows)
+// while the tensor core consumes the other, and one thread issues four
+// K=16 MMAs per slab and commits them to the stage's mbarrier.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w owns lanes
+// 32w..32w+31), applies bias / GELU / GELU' and stores.
+//
+// Every wait on an mbarrier is bounded: past the limit the kernel records
+// an error in *err, stops issuing work, waits (bounded again) for its own
+// MMAs, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/hexmlp.h"
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BK = 64;
+constexpr int THREADS = 128;
+constexpr uint32_t WAIT_LIMIT = 1u << 20;  // try_wait polls before an mbarrier wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
+// version 1; offsets in 16-byte units.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+
+// Bounded wait for the completion of phase `parity`; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// Copy a rows x 64 slab (K-contiguous rows of length ld) into the canonical
+// layout: chunk (r, kc) of 8 elements at (r/8)*1024 + kc*128 + (r%8)*16.
+__device__ __forceinline__ void load_slab(uint8_t* dst, const __nv_bfloat16* src, int rows, int ld, int k0) {
+  const int chunks = rows * (BK / 8);
+  for (int i = threadIdx.x; i < chunks; i += THREADS) {
+    const int r = i >> 3, kc = i & 7;
+    const uint4 v = *reinterpret_cast<const uint4*>(src + (size_t)r * ld + k0 + kc * 8);
+    *reinterpret_cast<uint4*>(dst + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16) = v;
+  }
+}
+
+using bf16 = __nv_bfloat16;
+
+// Kernel-side view of HexMlpGemm with typed pointers.
+struct Gemm {
+  const bf16* A;
+  const bf16* B;
+  int M, N, K, bn, epilogue;
+  const float* bias;
+  bf16* C;
+  bf16* Ct;
+  bf16* Z;
+  const bf16* Zin;
+  float* Cf;
+  int* err;
+};
+
+__global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int BN = p.bn;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nk = p.K / BK;
+  uint8_t* stage_a[2] = {smem, smem + BM * BK * 2};
+  uint8_t* stage_b[2] = {smem + 2 * BM * BK * 2, smem + 2 * BM * BK * 2 + BN * BK * 2};
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * BM * BK * 2 + 2 * BN * BK * 2);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  int& s_failed = *reinterpret_cast<int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    s_failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    // BN columns of tensor memory (128 or 256, a power of two as required)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc(BM, BN);
+
+  const __nv_bfloat16* A = p.A + (size_t)m0 * p.K;
+  const __nv_bfloat16* B = p.B + (size_t)n0 * p.K;
+  int issued = 0;  // slabs whose MMAs were issued
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt & 1;
+    if (kt >= 2) {
+      // the MMAs that read this stage (slab kt-2) must be done
+      if (threadIdx.x == 0 && !mbar_wait(smem_u32(&bars[s]), ((kt >> 1) - 1) & 1)) s_failed = 1;
+      __syncthreads();
+      if (s_failed) break;
+    }
+    load_slab(stage_a[s], A, BM, p.K, kt * BK);
+    load_slab(stage_b[s], B, BN, p.K, kt * BK);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(stage_a[s]), b0 = smem_u32(stage_b[s]);
+#pragma unroll
+      for (int j = 0; j < BK / 16; ++j) {
+        // K = 16 per MMA: two 8-element core-matrix columns, 256 bytes apart
+        const uint64_t ad = umma_desc(a0 + j * 256, 128, 1024);
+        const uint64_t bd = umma_desc(b0 + j * 256, 128, 1024);
+        mma_bf16(tmem, ad, bd, idesc, (kt > 0 || j > 0) ? 1u : 0u);
+      }
+      mma_commit(smem_u32(&bars[s]));
+    }
+    issued = kt + 1;
+  }
+  // wait for the last commit: every MMA issued before it is then complete
+  __syncthreads();
+  if (threadIdx.x == 0 && issued > 0) {
+    const int last = issued - 1;
+    if (!mbar_wait(smem_u32(&bars[last & 1]), (last >> 1) & 1)) s_failed = 1;
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const bool ok = s_failed == 0 && issued == nk;
+  if (!ok && threadIdx.x == 0) atomicOr(p.err, 1);
+
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < BN; c0 += 8) {
+      float v[8];
+      tmem_ld8(lane_base + (uint32_t)c0, v);
+      const int col = n0 + c0;
+      if (p.bias) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] += p.bias[col + i];
+      }
+      if (p.epilogue == HEXMLP_EPI_GELU) {
+        // Z (pre-activation) for the backward pass, H = GELU(Z) and H^T
+        __nv_bfloat16 z[8], h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          z[i] = __float2bfloat16_rn(v[i]);
+          h[i] = __float2bfloat16_rn(gelu(v[i]));
+        }
+        if (p.Z) *reinterpret_cast<uint4*>(p.Z + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(z);
+        if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(h);
+        if (p.Ct) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = h[i];
+        }
+      } else if (p.epilogue == HEXMLP_EPI_GELU_GRAD) {
+        // dZ = (dH) * GELU'(Z) with Z of this layer's forward pass
+        __nv_bfloat16 d[8];
+        const uint4 zr = *reinterpret_cast<const uint4*>(p.Zin + (size_t)row * p.N + col);
+        const __nv_bfloat16* zz = reinterpret_cast<const __nv_bfloat16*>(&zr);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zz[i])));
+        if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(d);
+        if (p.Ct) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = d[i];
+        }
+      } else {
+        // FP32 result (output layer, weight gradient)
+        float4* dst = reinterpret_cast<float4*>(p.Cf + (size_t)row * p.N + col);
+        dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+        dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+        if (p.C) {
+          __nv_bfloat16 b[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) b[i] = __float2bfloat16_rn(v[i]);
+          *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(b);
+        }
+      }
+    }
+  } else if (threadIdx.x == 0 && issued > 0) {
+    // gave up: a last bounded wait for this CTA's own MMAs before freeing
+    const int last = issued - 1;
+    mbar_wait(smem_u32(&bars[last & 1]), (last >> 1) & 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  }
+}
+
+// dY = 2 (Y - T) / count over the valid rows and columns (zero elsewhere),
+// in bf16 and transposed bf16; the squared error summed into *loss.
+__global__ void k_mse_grad(const float* __restrict__ Y, const float* __restrict__ T, int M, int N, int m_valid,
+                           int n_valid, float scale, __nv_bfloat16* __restrict__ dY,
+                           __nv_bfloat16* __restrict__ dYt, float* loss) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  float sq = 0.0f;
+  if (i < (size_t)M * N) {
+    const int m = (int)(i / N), n = (int)(i % N);
+    float g = 0.0f;
+    if (m < m_valid && n < n_valid) {
+      const float d = Y[i] - T[i];
+      sq = d * d;
+      g = 2.0f * d * scale;
+    }
+    const __nv_bfloat16 b = __float2bfloat16_rn(g);
+    dY[i] = b;
+    if (dYt) dYt[(size_t)n * M + m] = b;
+  }
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, sq);
+}
+
+// db[n] = sum over m of dZ^T[n][m]
+__global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dZt, int N, int M, float* __restrict__ db) {
+  const int n = blockIdx.x;
+  float acc = 0.0f;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) acc += __bfloat162float(dZt[(size_t)n * M + m]);
+  __shared__ float red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) db[n] = acc;
+  }
+}
+
+// Adam on FP32 master weights [rows][cols] (bias when rows == 1); refreshes
+// the bf16 copy and, when given, its transpose.
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m1, float* __restrict__ m2,
+                       const float* __restrict__ g, int rows, int cols, float lr, float b1, float b2, float eps,
+                       float c1, float c2, float decay, __nv_bfloat16* __restrict__ wb, __nv_bfloat16* __restrict__ wbt) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)rows * cols) return;
+  const float gi = g[i] + decay * w[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  const float wi = w[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+  w[i] = wi;
+  const __nv_bfloat16 h = __float2bfloat16_rn(wi);
+  if (wb) wb[i] = h;
+  if (wbt) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    wbt[(size_t)c * rows + r] = h;
+  }
+}
+
+// out[r][f] = bf16((raw[r][f] - mean[f]) * inv_std[f]) for r < rows and
+// f < n_feat, zero elsewhere in [rows_pad][ld_out]; the transpose too if given.
+__global__ void k_pack(const float* __restrict__ raw, int rows, int n_feat, int ld_raw,
+                       const float* __restrict__ mean, const float* __restrict__ inv_std, int rows_pad, int ld_out,
+                       bf16* __restrict__ out, bf16* __restrict__ out_t) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)rows_pad * ld_out) return;
+  const int r = (int)(i / ld_out), f = (int)(i % ld_out);
+  float v = 0.0f;
+  if (r < rows && f < n_feat) v = (raw[(size_t)r * ld_raw + f] - mean[f]) * inv_std[f];
+  const bf16 b = __float2bfloat16_rn(v);
+  out[i] = b;
+  if (out_t) out_t[(size_t)f * rows_pad + r] = b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hexmlp_pack(const float* raw, int rows, int n_feat, int ld_raw, const float* mean, const float* inv_std,
+                int rows_pad, int ld_out, void* out, void* out_t, void* stream) {
+  if (!raw || !mean || !inv_std || !out || rows < 0 || rows > rows_pad || n_feat > ld_out || n_feat > ld_raw)
+    return HEXMLP_E_ARG;
+  const size_t n = (size_t)rows_pad * ld_out;
+  if (n == 0) return 0;
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(raw, rows, n_feat, ld_raw, mean, inv_std,
+                                                                       rows_pad, ld_out, (bf16*)out, (bf16*)out_t);
+  return (int)cudaGetLastError();
+}
+
+size_t hexmlp_gemm_smem_bytes(int bn) { return (size_t)2 * BM * BK * 2 + (size_t)2 * bn * BK * 2 + 64; }
+
+int hexmlp_gemm_tile_rows(void) { return BM; }
+int hexmlp_gemm_tile_k(void) { return BK; }
+
+int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
+  if (!p || !p->A || !p->B || !p->err) return HEXMLP_E_ARG;
+  if (p->M <= 0 || p->N <= 0 || p->K <= 0 || p->M % BM || p->K % BK) return HEXMLP_E_ARG;
+  if (!(p->bn == 128 || p->bn == 256) || p->N % p->bn) return HEXMLP_E_ARG;
+  if (p->epilogue == HEXMLP_EPI_F32 && !p->Cf) return HEXMLP_E_ARG;
+  if (p->epilogue == HEXMLP_EPI_GELU_GRAD && !p->Zin) return HEXMLP_E_ARG;
+  if (p->epilogue < HEXMLP_EPI_F32 || p->epilogue > HEXMLP_EPI_GELU_GRAD) return HEXMLP_E_ARG;
+  // 16-byte alignment of every row: K and N multiples of 8 hold by the checks
+  // above; the base pointers must be 16-byte aligned
+  const void* ptrs[] = {p->A, p->B, p->C, p->Z, p->Zin, p->Cf};
+  for (const void* q : ptrs)
+    if (q && ((uintptr_t)q & 15u)) return HEXMLP_E_ARG;
+  const size_t smem = hexmlp_gemm_smem_bytes(p->bn);
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return (int)e;
+  const Gemm g{(const bf16*)p->A, (const bf16*)p->B, p->M, p->N, p->K, p->bn, p->epilogue, p->bias, (bf16*)p->C,
+               (bf16*)p->Ct, (bf16*)p->Z, (const bf16*)p->Zin, p->Cf, p->err};
+  dim3 grid(p->M / BM, p->N / p->bn);
+  k_gemm_bf16<<<grid, THREADS, smem, (cudaStream_t)stream>>>(g);
+  return (int)cudaGetLastError();
+}
+
+int hexmlp_mse_grad(const float* Y, const float* T, int M, int N, int m_valid, int n_valid, float scale,
+                    void* dY_, void* dYt_, float* loss, void* stream) {
+  bf16* dY = (bf16*)dY_;
+  bf16* dYt = (bf16*)dYt_;
+  if (!Y || !T || !dY || M <= 0 || N <= 0) return HEXMLP_E_ARG;
+  const size_t n = (size_t)M * N;
+  k_mse_grad<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(Y, T, M, N, m_valid, n_valid, scale,
+                                                                          dY, dYt, loss);
+  return (int)cudaGetLastError();
+}
+
+int hexmlp_bias_grad(const void* dZt_, int N, int M, float* db, void* stream) {
+  const bf16* dZt = (const bf16*)dZt_;
+  if (!dZt || !db || N <= 0 || M <= 0) return HEXMLP_E_ARG;
+  k_bias_grad<<<N, 256, 0, (cudaStream_t)stream>>>(dZt, N, M, db);
+  return (int)cudaGetLastError();
+}
+
+int hexmlp_adam(float* w, float* m1, float* m2, const float* g, int rows, int cols, float lr, float b1, float b2,
+                float eps, int t, float decay, void* wb_, void* wbt_, void* stream) {
+  bf16* wb = (bf16*)wb_;
+  bf16* wbt = (bf16*)wbt_;
+  if (!w || !m1 || !m2 || !g || rows <= 0 || cols <= 0 || t < 1) return HEXMLP_E_ARG;
+  const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
+  const size_t n = (size_t)rows * cols;
+  k_adam<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(w, m1, m2, g, rows, cols, lr, b1, b2, eps,
+                                                                      c1, c2, decay, wb, wbt);
+  return (int)cudaGetLastError();
+}
+
+}  // extern "C"

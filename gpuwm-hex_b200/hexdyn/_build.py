@@ -26,6 +26,7 @@ UNITS = {
     "kernels_strict.cu": ["-fmad=false"],
     "kernels_fast.cu": ["-fmad=true"],
     "hexdyn_abi.cu": ["-fmad=false"],
+    "mlp_umma.cu": [],
 }
 
 

@@ -91,6 +91,11 @@ EXPORTS = {
     "hexdyn_set_member_state": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F32P, C.c_size_t, C.c_void_p]),
     "hexdyn_get_member_state": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F32P, C.c_size_t, C.c_void_p]),
     "hexdyn_step_batched": (C.c_int, [C.POINTER(HexDynBatch), C.c_void_p]),
+    "hexdyn_column_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "hexdyn_edge_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "hexdyn_apply_increments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hexdyn_total_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -237,6 +237,28 @@ typedef struct HexDynBatch {
  * naming the first group; with flags == NULL nothing synchronises. */
 int hexdyn_step_batched(const HexDynBatch* batch, void* stream);
 
+/* Learned-corrector state access (no counterpart in the reference: the
+ * corrector is this library's own).  All act on the current state of `h`
+ * and are enqueued on `stream`; arrays are device pointers.
+ *   hexdyn_column_features: X [n_cells][ld] floats, ld >= 6 L: theta_m,
+ *     rho_zz, w (interfaces 0..L-1), first scalar, mean u over the cell's
+ *     edges, mean theta_m over the neighbouring cells, each over L levels.
+ *   hexdyn_edge_features: X [n_edges][ld], ld >= 4 L: u, theta_m of both
+ *     cells, mean rho_zz of both cells.
+ *   hexdyn_apply_increments: adds y * scale + shift (per feature) of the
+ *     column outputs (theta_m, rho_zz, w; [n_cells][ldc]) and of the edge
+ *     outputs (u; [n_edges][lde]) to the prognostic state; either may be
+ *     NULL.  Rebuild the saved diagnostics afterwards.
+ *   hexdyn_total_energy: dev_out[0] (device double) = internal + potential
+ *     + kinetic energy, dev_out[1] = the volume integral of w^2, with z_mid
+ *     the height of every cell level in the padded [cell][level] layout. */
+int hexdyn_column_features(HexDynHandle* h, float* X, int ld, void* stream);
+int hexdyn_edge_features(HexDynHandle* h, float* X, int ld, void* stream);
+int hexdyn_apply_increments(HexDynHandle* h, const float* Ycol, int ldc, const float* col_scale,
+                            const float* col_shift, const float* Yedge, int lde, const float* edge_scale,
+                            const float* edge_shift, void* stream);
+int hexdyn_total_energy(HexDynHandle* h, const float* z_mid, double* dev_out, void* stream);
+
 /* Copy the last error message of this thread into buf. */
 int hexdyn_last_error(char* buf, size_t len);
 

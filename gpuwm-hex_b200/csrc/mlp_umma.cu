@@ -9,16 +9,21 @@
 // gradient, H^T and dZ^T for the weight gradient), so one kernel serves the
 // forward pass and both backward products.
 //
-// Tiling: a CTA of 128 threads owns a 128 x BN output tile (BN = 128 or
+// Tiling: a CTA of 256 threads owns a 128 x BN output tile (BN = 128 or
 // 256) whose FP32 accumulator lives in BN columns of tensor memory (128
-// lanes = 128 rows).  K advances in 64-element slabs through two shared
-// memory stages; the threads fill a stage with 16-byte loads in the
+// lanes = 128 rows).  K advances in 64-element slabs through NSTAGE shared
+// memory stages filled by asynchronous 16-byte copies (cp.async) in the
 // canonical K-major no-swizzle layout (8-row x 16-byte core matrices; the
-// descriptor's leading offset steps along K, the stride offset along rows)
-// while the tensor core consumes the other, and one thread issues four
-// K=16 MMAs per slab and commits them to the stage's mbarrier.  The
-// epilogue reads the accumulator with tcgen05.ld (warp w owns lanes
-// 32w..32w+31), applies bias / GELU / GELU' and stores.
+// descriptor's leading offset steps along K, the stride offset along rows):
+// the copies of the next NSTAGE-1 slabs are in flight while the tensor core
+// works on the current one.  One thread issues four K=16 MMAs per slab and
+// commits them to the stage's mbarrier; a stage is refilled once that
+// mbarrier completes.  The epilogue reads the accumulator with tcgen05.ld
+// (warp w may read lanes 32(w%4)..32(w%4)+31, so warps w and w+4 split that
+// lane quarter's columns in halves), applies bias / GELU / GELU' and stores.
+//
+// GELU is the tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))),
+// evaluated with the hardware tanh approximation (tanh.approx.f32).
 //
 // Every wait on an mbarrier is bounded: past the limit the kernel records
 // an error in *err, stops issuing work, waits (bounded again) for its own
@@ -34,7 +39,8 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 64;
-constexpr int THREADS = 128;
+constexpr int THREADS = 256;
+constexpr int NSTAGE = 3;
 constexpr uint32_t WAIT_LIMIT = 1u << 20;  // try_wait polls before an mbarrier wait gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -91,30 +97,53 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
-  uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
+// 32 consecutive accumulator columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.0f + tanh_hw(GELU_C * (x + GELU_A * x * x * x)));
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float t = tanh_hw(GELU_C * (x + GELU_A * x * x * x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_C * (1.0f + 3.0f * GELU_A * x * x);
 }
 
-// Copy a rows x 64 slab (K-contiguous rows of length ld) into the canonical
-// layout: chunk (r, kc) of 8 elements at (r/8)*1024 + kc*128 + (r%8)*16.
+// Asynchronous copy of a rows x 64 slab (K-contiguous rows of length ld)
+// into the canonical layout: chunk (r, kc) of 8 elements at
+// (r/8)*1024 + kc*128 + (r%8)*16.
 __device__ __forceinline__ void load_slab(uint8_t* dst, const __nv_bfloat16* src, int rows, int ld, int k0) {
   const int chunks = rows * (BK / 8);
   for (int i = threadIdx.x; i < chunks; i += THREADS) {
     const int r = i >> 3, kc = i & 7;
-    const uint4 v = *reinterpret_cast<const uint4*>(src + (size_t)r * ld + k0 + kc * 8);
-    *reinterpret_cast<uint4*>(dst + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16) = v;
+    const void* g = src + (size_t)r * ld + k0 + kc * 8;
+    const uint32_t d = smem_u32(dst + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
   }
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 using bf16 = __nv_bfloat16;
@@ -133,21 +162,21 @@ struct Gemm {
   int* err;
 };
 
-__global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
+__global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int BN = p.bn;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int nk = p.K / BK;
-  uint8_t* stage_a[2] = {smem, smem + BM * BK * 2};
-  uint8_t* stage_b[2] = {smem + 2 * BM * BK * 2, smem + 2 * BM * BK * 2 + BN * BK * 2};
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * BM * BK * 2 + 2 * BN * BK * 2);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  const int stage_bytes = (BM + BN) * BK * 2;
+  auto stage_a = [&](int s) { return smem + s * stage_bytes; };
+  auto stage_b = [&](int s) { return smem + s * stage_bytes + BM * BK * 2; };
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + NSTAGE * stage_bytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + NSTAGE);
   int& s_failed = *reinterpret_cast<int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    mbar_init(smem_u32(&bars[0]), 1);
-    mbar_init(smem_u32(&bars[1]), 1);
+    for (int s = 0; s < NSTAGE; ++s) mbar_init(smem_u32(&bars[s]), 1);
     s_failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -166,21 +195,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
   const __nv_bfloat16* A = p.A + (size_t)m0 * p.K;
   const __nv_bfloat16* B = p.B + (size_t)n0 * p.K;
   int issued = 0;  // slabs whose MMAs were issued
-  for (int kt = 0; kt < nk; ++kt) {
-    const int s = kt & 1;
-    if (kt >= 2) {
-      // the MMAs that read this stage (slab kt-2) must be done
-      if (threadIdx.x == 0 && !mbar_wait(smem_u32(&bars[s]), ((kt >> 1) - 1) & 1)) s_failed = 1;
-      __syncthreads();
-      if (s_failed) break;
+  // prologue: the first NSTAGE-1 slabs in flight (one commit group each)
+  for (int q = 0; q < NSTAGE - 1; ++q) {
+    if (q < nk) {
+      load_slab(stage_a(q), A, BM, p.K, q * BK);
+      load_slab(stage_b(q), B, BN, p.K, q * BK);
     }
-    load_slab(stage_a[s], A, BM, p.K, kt * BK);
-    load_slab(stage_b[s], B, BN, p.K, kt * BK);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt % NSTAGE;
+    cp_wait<NSTAGE - 2>();  // this thread's copies of slab kt have landed
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(stage_a[s]), b0 = smem_u32(stage_b[s]);
+      const uint32_t a0 = smem_u32(stage_a(s)), b0 = smem_u32(stage_b(s));
 #pragma unroll
       for (int j = 0; j < BK / 16; ++j) {
         // K = 16 per MMA: two 8-element core-matrix columns, 256 bytes apart
@@ -191,12 +221,25 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
       mma_commit(smem_u32(&bars[s]));
     }
     issued = kt + 1;
+    // refill the stage of slab kt-1 with slab kt+NSTAGE-1 once slab kt-1's
+    // MMAs (committed one iteration ago) are complete
+    const int nxt = kt + NSTAGE - 1;
+    if (nxt < nk) {
+      const int sn = nxt % NSTAGE;
+      if (kt >= 1 && threadIdx.x == 0 && !mbar_wait(smem_u32(&bars[sn]), ((kt - 1) / NSTAGE) & 1)) s_failed = 1;
+      __syncthreads();
+      if (s_failed) break;
+      load_slab(stage_a(sn), A, BM, p.K, nxt * BK);
+      load_slab(stage_b(sn), B, BN, p.K, nxt * BK);
+    }
+    cp_commit();
   }
+  cp_wait<0>();
   // wait for the last commit: every MMA issued before it is then complete
   __syncthreads();
   if (threadIdx.x == 0 && issued > 0) {
     const int last = issued - 1;
-    if (!mbar_wait(smem_u32(&bars[last & 1]), (last >> 1) & 1)) s_failed = 1;
+    if (!mbar_wait(smem_u32(&bars[last % NSTAGE]), (last / NSTAGE) & 1)) s_failed = 1;
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -204,12 +247,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
   if (!ok && threadIdx.x == 0) atomicOr(p.err, 1);
 
   if (ok) {
-    const int row = m0 + warp * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < BN; c0 += 8) {
-      float v[8];
-      tmem_ld8(lane_base + (uint32_t)c0, v);
-      const int col = n0 + c0;
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = m0 + quarter * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    for (int c32 = half * (BN / 2); c32 < (half + 1) * (BN / 2); c32 += 32) {
+      float v32[32];
+      tmem_ld32(lane_base + (uint32_t)c32, v32);
+#pragma unroll
+      for (int g8 = 0; g8 < 4; ++g8) {
+      float* v = v32 + 8 * g8;
+      const int col = n0 + c32 + 8 * g8;
       if (p.bias) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) v[i] += p.bias[col + i];
@@ -252,11 +299,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_bf16(Gemm p) {
           *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(b);
         }
       }
+      }
     }
   } else if (threadIdx.x == 0 && issued > 0) {
     // gave up: a last bounded wait for this CTA's own MMAs before freeing
     const int last = issued - 1;
-    mbar_wait(smem_u32(&bars[last & 1]), (last >> 1) & 1);
+    mbar_wait(smem_u32(&bars[last % NSTAGE]), (last / NSTAGE) & 1);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -357,7 +405,7 @@ int hexmlp_pack(const float* raw, int rows, int n_feat, int ld_raw, const float*
   return (int)cudaGetLastError();
 }
 
-size_t hexmlp_gemm_smem_bytes(int bn) { return (size_t)2 * BM * BK * 2 + (size_t)2 * bn * BK * 2 + 64; }
+size_t hexmlp_gemm_smem_bytes(int bn) { return (size_t)NSTAGE * (BM + bn) * BK * 2 + 64; }
 
 int hexmlp_gemm_tile_rows(void) { return BM; }
 int hexmlp_gemm_tile_k(void) { return BK; }

@@ -77,8 +77,10 @@ def round_up(x: int, m: int) -> int:
     return (x + m - 1) // m * m
 
 
-def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=None, Zin=None, Cf=None, err=None):
-    """C = A . B^T on the tensor cores (see include/hexmlp.h)."""
+def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=None, Zin=None, Cf=None, err=None,
+         bn: int = 128):
+    """C = A . B^T on the tensor cores (see include/hexmlp.h).  ``bn``: the
+    output tile width, 128 (two CTAs per SM, the default) or 256."""
     import torch
 
     M, K = A.shape
@@ -87,7 +89,6 @@ def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=Non
     assert A.is_contiguous() and B.is_contiguous()
     if err is None:
         err = torch.zeros(1, dtype=torch.int32, device=A.device)
-    bn = 256 if N % 256 == 0 else 128
     p = HexMlpGemm(_ptr(A), _ptr(B), M, N, K, bn, epilogue, _ptr(bias), _ptr(C_out), _ptr(Ct), _ptr(Z), _ptr(Zin),
                    _ptr(Cf), _ptr(err))
     _check(load().hexmlp_gemm(C.byref(p), _stream()), f"hexmlp_gemm {M}x{N}x{K}")
@@ -223,3 +224,44 @@ class TensorCoreMLP:
     def check(self) -> None:
         if int(self.err.item()) != 0:
             raise RuntimeError("a tensor-core GEMM gave up waiting on its MMAs")
+
+
+def forward_flops(net: TensorCoreMLP, M: int) -> float:
+    """FLOPs of one forward pass over M rows at the padded layer widths."""
+    dims = [net.p_in] + [net.p_hidden] * net.depth + [net.p_out]
+    return 2.0 * M * sum(a * b for a, b in zip(dims[:-1], dims[1:]))
+
+
+def bench_forward(n_in: int = 330, hidden: int = 512, depth: int = 3, n_out: int = 165, rows: int = 40962,
+                  reps: int = 20) -> dict:
+    """Time the forward pass of a network over ``rows`` rows (the column
+    network over every column of the 40962-cell mesh by default) with CUDA
+    events; returns milliseconds and TFLOP/s at the padded widths."""
+    import torch
+
+    net = TensorCoreMLP(n_in, hidden, depth, n_out, seed=0)
+    M = round_up(rows, TILE_M)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn(M, net.p_in, device="cuda", generator=gen).to(torch.bfloat16)
+    for _ in range(3):
+        net.forward(X)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(X)
+    e1.record()
+    torch.cuda.synchronize()
+    net.check()
+    ms = e0.elapsed_time(e1) / reps
+    flops = forward_flops(net, M)
+    return {"rows": M, "shape": f"{net.p_in} -> {net.p_hidden} x{depth} -> {net.p_out}", "ms": ms,
+            "tflops": flops / (ms / 1000.0) / 1e12, "gemm_launches": depth + 1}
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    if len(sys.argv) > 1 and sys.argv[1] == "--bench":
+        print(json.dumps({"column": bench_forward(), "edge": bench_forward(220, 256, 3, 55, rows=122880)}))

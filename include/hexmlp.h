@@ -24,7 +24,8 @@ extern "C" {
 
 /* GEMM epilogues. */
 #define HEXMLP_EPI_F32 0        /* Cf = A.B^T (+ bias); optional bf16 copy in C */
-#define HEXMLP_EPI_GELU 1       /* Z = A.B^T + bias (bf16), C = GELU(Z), Ct = C^T */
+#define HEXMLP_EPI_GELU 1       /* Z = A.B^T + bias (bf16), C = GELU(Z), Ct = C^T; GELU in
+                                   its tanh form with the hardware tanh approximation */
 #define HEXMLP_EPI_GELU_GRAD 2  /* C = (A.B^T) * GELU'(Zin), Ct = C^T (bf16) */
 
 /* C[M][N] = A[M][K] . B[N][K]^T; A and B bf16 with K contiguous.  M a

@@ -54,8 +54,8 @@ def _bf(x):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N", [384, 512])
-def test_gemm_epilogues_match_float64(N):
+@pytest.mark.parametrize("N,bn", [(384, 128), (512, 256)])
+def test_gemm_epilogues_match_float64(N, bn):
     from hexdyn import mlp
 
     assert torch.cuda.is_available()
@@ -67,7 +67,7 @@ def test_gemm_epilogues_match_float64(N):
     ref = A.astype(np.float64) @ B.astype(np.float64).T
     At, Bt = _bf(A), _bf(B)
     Cf = torch.empty(M, N, dtype=torch.float32, device="cuda")
-    err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf)
+    err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf, bn=bn)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     np.testing.assert_allclose(Cf.cpu().numpy(), ref, rtol=0, atol=1e-4 * np.abs(ref).max())
@@ -75,7 +75,7 @@ def test_gemm_epilogues_match_float64(N):
     H = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
     Ht = torch.empty(N, M, dtype=torch.bfloat16, device="cuda")
     Z = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
-    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU, bias=torch.from_numpy(bias).cuda(), C_out=H, Ct=Ht, Z=Z, err=err)
+    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU, bias=torch.from_numpy(bias).cuda(), C_out=H, Ct=Ht, Z=Z, err=err, bn=bn)
     z = ref + bias
     np.testing.assert_allclose(Z.float().cpu().numpy(), z, rtol=1e-2, atol=1e-2)
     h = om.gelu(z)
@@ -84,7 +84,7 @@ def test_gemm_epilogues_match_float64(N):
     # GELU' epilogue on a given Z
     D = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
     Dt = torch.empty(N, M, dtype=torch.bfloat16, device="cuda")
-    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU_GRAD, C_out=D, Ct=Dt, Zin=Z, err=err)
+    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU_GRAD, C_out=D, Ct=Dt, Zin=Z, err=err, bn=bn)
     want = ref * om.gelu_grad(Z.float().cpu().numpy())
     np.testing.assert_allclose(D.float().cpu().numpy(), want, rtol=1e-2, atol=1e-2 * np.abs(want).max())
     np.testing.assert_array_equal(Dt.float().cpu().numpy(), D.float().cpu().numpy().T)

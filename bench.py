@@ -50,6 +50,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--condensates", type=int, default=5)
     ap.add_argument("--numerics", default="strict", choices=["strict", "fast"])
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--autotune", default="on", choices=["on", "off"],
+                    help="choose the block size of every kernel by timing before capturing the graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
     ap.add_argument("--batched", default="on", choices=["on", "off"],
@@ -279,8 +281,11 @@ def run_ensemble(args, stream, dist, world: int, rank: int, plain_case) -> dict:
         return ms
 
     # looped: every member its own single-instance driver (whole step as a graph)
-    singles = [(hexdyn.from_case(c, cfgs[gi], capture_graph=True), per)
-               for gi, (sel, per) in enumerate(my_groups) for c in sel]
+    singles = [(hexdyn.from_case(c, cfgs[gi]), per) for gi, (sel, per) in enumerate(my_groups) for c in sel]
+    for drv, _ in singles:
+        if args.autotune == "on":
+            drv.autotune(1)
+        drv.capture_graph()
 
     def looped():
         for drv, per in singles:
@@ -293,8 +298,11 @@ def run_ensemble(args, stream, dist, world: int, rank: int, plain_case) -> dict:
         drv.close()
     del singles
     # batched: one ensemble per time step, both groups per call
-    ens = [(HexEnsemble.from_cases(sel, cfgs[gi], capture_graph=True), per)
-           for gi, (sel, per) in enumerate(my_groups) if sel]
+    ens = [(HexEnsemble.from_cases(sel, cfgs[gi]), per) for gi, (sel, per) in enumerate(my_groups) if sel]
+    for e, _ in ens:
+        if args.autotune == "on":
+            e.autotune(1)
+        e.capture_graph()
 
     def batched():
         step_batched([e for e, _ in ens], [per for _, per in ens], read_flags=False, stream=stream)
@@ -383,7 +391,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     case = build_workload(args)
     cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=2, moist_coefficients="native",
                        numerics=args.numerics)
-    drv = hexdyn.from_case(case, cfg, capture_graph=not args.no_graph)
+    drv = hexdyn.from_case(case, cfg)
+    tuning = drv.autotune(2) if args.autotune == "on" else {}
+    if not args.no_graph:
+        drv.capture_graph()
     stream = torch.cuda.current_stream()
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[0])
                            if world == 1 else local_rank).start()
@@ -512,6 +523,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                          "traffic": traffic, "bytes_per_launch": dk["bytes"], "avg_launch_us": dk["avg_us"],
                          "share": dk["share"]},
+            "autotune": {k: v["threads"] for k, v in tuning.items()},
             "step_bytes_algorithmic": step_bytes,
             "step_gbs": step_bytes / (ms_per_step / 1000.0) / 1e9,
             "kernels": kernels,

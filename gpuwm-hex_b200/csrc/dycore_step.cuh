@@ -8,7 +8,11 @@ struct Launcher {
   std::vector<HexProfEvent>* prof = nullptr;  // per-launch CUDA events when profiling
   long long count = 0;
   cudaError_t err = cudaSuccess;
-  int epb(int tpe) const { return tpe >= 256 ? 1 : 256 / tpe; }
+  // entities per block for tpe threads per entity under the label's block size
+  int epb(const char* name, int tpe) const {
+    const int threads = ctx.threads_for(name);
+    return tpe >= threads ? 1 : threads / tpe;
+  }
   template <class K, class... A>
   void lp(const char* name, int n, int nz, size_t smem_per_entity, K kernel, A... args) {
     launch(name, ctx.geo.S, n, nz, smem_per_entity, kernel, args...);
@@ -42,7 +46,7 @@ struct Launcher {
   void launch_impl(const char* name, int tpe, int n, int nz, size_t smem_per_entity, bool fold, K kernel,
                    A... args) {
     if (err != cudaSuccess || n <= 0 || nz <= 0) return;
-    const int e = epb(tpe);
+    const int e = epb(name, tpe);
     const unsigned nb = (unsigned)((n + e - 1) / e);
     dim3 block(tpe, e), grid(fold ? nb * (unsigned)nz : nb, 1, fold ? 1 : nz);
     HexProfEvent ev{name, nullptr, nullptr};

@@ -630,6 +630,117 @@ int hexdyn_profile_steps(HexDynHandle* h, void* stream, int nsteps, char* out, s
   return text.size() < len ? HEXDYN_OK : fail(HEXDYN_E_CAPACITY, "profile text needs %zu bytes", text.size() + 1);
 }
 
+// Per-label mean launch time (ms) of nsteps eager steps, one CUDA event pair
+// per launch.
+static cudaError_t profile_means(HexDynHandle* h, cudaStream_t st, int nsteps,
+                                 std::vector<std::pair<std::string, double>>& out) {
+  std::vector<HexProfEvent> prof;
+  prof.reserve(4096);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
+    e = enqueue_step(h, st, &prof);
+    h->ctx.parity ^= 1;
+  }
+  cudaError_t se = cudaStreamSynchronize(st);
+  std::vector<long long> count;
+  out.clear();
+  for (auto& ev : prof) {
+    float ms = 0.0f;
+    if (e == cudaSuccess && se == cudaSuccess) cudaEventElapsedTime(&ms, ev.start, ev.stop);
+    size_t i = 0;
+    while (i < out.size() && out[i].first != ev.name) ++i;
+    if (i == out.size()) {
+      out.emplace_back(ev.name, 0.0);
+      count.push_back(0);
+    }
+    out[i].second += ms;
+    count[i] += 1;
+    cudaEventDestroy(ev.start);
+    cudaEventDestroy(ev.stop);
+  }
+  for (size_t i = 0; i < out.size(); ++i) out[i].second /= (double)count[i];
+  return e != cudaSuccess ? e : se;
+}
+
+int hexdyn_autotune(HexDynHandle* h, void* stream, int steps_per_candidate, char* report, size_t len) {
+  if (!h || steps_per_candidate < 1) return fail(HEXDYN_E_ARG, "NULL handle or steps_per_candidate < 1");
+  for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f)
+    if (!h->have_state[f] && !(f == HEXDYN_SCALARS && h->ctx.n_scalars == 0))
+      return fail(HEXDYN_E_STATE, "state field %d was never set", f);
+  HexCtx& c = h->ctx;
+  cudaStream_t st = (cudaStream_t)stream;
+  // save the current state and sidecar; every candidate starts from it
+  struct Saved { float* dev; float* copy; size_t bytes; };
+  std::vector<Saved> saved;
+  const HexState s0 = cur_state(h);
+  const HexSide d0 = cur_side(h);
+  for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f) {
+    const FieldShape fs = field_shape(c, f);
+    const size_t words = (size_t)fs.blocks * fs.n * c.geo.S;
+    float* dev = field_ptr(s0, d0, f);
+    if (!dev || words == 0) continue;
+    void* copy = nullptr;
+    cudaError_t e = cudaMalloc(&copy, words * sizeof(float));
+    if (e != cudaSuccess) {
+      for (auto& x : saved) cudaFree(x.copy);
+      return cuda_fail(e, "autotune state copy");
+    }
+    saved.push_back({dev, (float*)copy, words * sizeof(float)});
+    cudaMemcpyAsync(copy, dev, words * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  }
+  const int parity0 = c.parity;
+  auto restore = [&]() {
+    c.parity = parity0;
+    for (auto& x : saved) cudaMemcpyAsync(x.dev, x.copy, x.bytes, cudaMemcpyDeviceToDevice, st);
+  };
+  const int candidates[3] = {64, 128, 256};
+  std::vector<std::pair<std::string, double>> times[3];
+  cudaError_t err = cudaSuccess;
+  for (int ci = 0; ci < 3 && err == cudaSuccess; ++ci) {
+    restore();
+    c.force_threads = candidates[ci];
+    err = profile_means(h, st, steps_per_candidate, times[ci]);
+  }
+  c.force_threads = 0;
+  restore();
+  cudaError_t se = cudaStreamSynchronize(st);
+  for (auto& x : saved) cudaFree(x.copy);
+  cudaMemsetAsync(c.w.flag, 0, sizeof(int), st);
+  if (err != cudaSuccess) return cuda_fail(err, "autotune step");
+  if (se != cudaSuccess) return cuda_fail(se, "autotune restore");
+  // the fastest block size of every label
+  std::string text;
+  std::vector<std::pair<std::string, int>> tuned;
+  for (const auto& lab : times[2]) {
+    double best = 1e30;
+    int best_t = 256;
+    double t3[3] = {0.0, 0.0, 0.0};
+    for (int ci = 0; ci < 3; ++ci)
+      for (const auto& x : times[ci])
+        if (x.first == lab.first) {
+          t3[ci] = x.second;
+          if (x.second < best) {
+            best = x.second;
+            best_t = candidates[ci];
+          }
+        }
+    tuned.emplace_back(lab.first, best_t);
+    char line[256];
+    snprintf(line, sizeof line, "%s %.3f %.3f %.3f %d\n", lab.first.c_str(), 1000.0 * t3[0], 1000.0 * t3[1],
+             1000.0 * t3[2], best_t);
+    text += line;
+  }
+  c.tuned_threads = tuned;
+  // captured graphs hold the old launch shapes
+  if (c.graph_exec[0] || c.graph_exec[1]) {
+    const int rc = hexdyn_capture_graph(h, stream);
+    if (rc) return rc;
+  }
+  if (report && len) snprintf(report, len, "%s", text.c_str());
+  return (report && len && text.size() >= len) ? fail(HEXDYN_E_CAPACITY, "report needs %zu bytes", text.size() + 1)
+                                               : HEXDYN_OK;
+}
+
 int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out) {
   if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
   cudaStream_t st = (cudaStream_t)stream;

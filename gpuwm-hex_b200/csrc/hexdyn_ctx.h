@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "dycore_geo.cuh"
@@ -78,6 +79,17 @@ struct HexCtx {
   int parity = 0;       // 0: state in `in`, 1: state in `out`
   long long steps_done = 0;
   long long launches_per_step = 0;
+  // Autotuned block size (threads) per launch label; labels not listed use
+  // 256 threads, and `force_threads` (when non-zero) overrides every label
+  // while the autotuner times a candidate.
+  std::vector<std::pair<std::string, int>> tuned_threads;
+  int force_threads = 0;
+  int threads_for(const char* label) const {
+    if (force_threads) return force_threads;
+    for (const auto& t : tuned_threads)
+      if (t.first == label) return t.second;
+    return 256;
+  }
 };
 
 namespace hexdyn_strict {

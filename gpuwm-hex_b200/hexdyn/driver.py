@@ -236,6 +236,19 @@ class HexDycoreDriver:
         _lib.check(self._lib.hexdyn_capture_graph(self._handle, self._stream_handle()))
         self._graph = True
 
+    def autotune(self, steps_per_candidate: int = 2) -> dict[str, dict]:
+        """Choose the block size of every kernel launch by timing (see
+        ``hexdyn_autotune``); the state is left as it was.  Returns, per
+        launch label, the microseconds at 64/128/256 threads and the choice."""
+        buf = C.create_string_buffer(1 << 16)
+        _lib.check(self._lib.hexdyn_autotune(self._handle, self._stream_handle(), int(steps_per_candidate), buf,
+                                             len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, t64, t128, t256, chosen = line.split()
+            out[name] = {"us": {64: float(t64), 128: float(t128), 256: float(t256)}, "threads": int(chosen)}
+        return out
+
     # -------------------------------------------------------------- steps
     def step_async(self, nsteps: int = 1) -> None:
         _lib.check(self._lib.hexdyn_step_async(self._handle, self._stream_handle(), int(nsteps)))

@@ -162,6 +162,16 @@ int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out);
  * hexcore/cuda_subcycle_graphs.py:45-62.) */
 int hexdyn_profile_steps(HexDynHandle* h, void* stream, int nsteps, char* out, size_t len);
 
+/* Autotuner of launch shapes (no counterpart in the reference, whose
+ * kernels launch fixed shapes): times every kernel of `steps_per_candidate`
+ * eager steps with 64, 128 and 256 threads per block (CUDA events per
+ * launch), keeps the fastest block size of every launch label, and restores
+ * the state and sidecar the steps started from; captured graphs are
+ * captured again with the tuned shapes.  Results do not depend on the block
+ * size (every entity is computed by the same code).  `report` receives one
+ * line per label: "label us@64 us@128 us@256 chosen". */
+int hexdyn_autotune(HexDynHandle* h, void* stream, int steps_per_candidate, char* report, size_t len);
+
 /* Capture the whole large step into CUDA graphs (one per buffer parity);
  * later hexdyn_step calls replay them. */
 int hexdyn_capture_graph(HexDynHandle* h, void* stream);

@@ -26,6 +26,11 @@ struct HexDynHandle {
   // each member has been given
   std::vector<int> m_c0, m_e0, m_v0, m_nc, m_ne, m_nv;
   std::vector<unsigned> m_have;
+  // the library's own buffers of the parity-0 state while caller buffers are
+  // bound (hexdyn_bind_state)
+  bool bound = false;
+  HexState own_in{};
+  HexSide own_side_in{};
   // private stream and events of hexdyn_step_batched
   cudaStream_t batch_stream = nullptr;
   cudaEvent_t batch_fork = nullptr, batch_done = nullptr;
@@ -1336,6 +1341,48 @@ int hexdyn_total_energy(HexDynHandle* h, const float* z_mid, double* dev_out, vo
 
 }  // extern "C"
 
+// ------------------------------------------------------------- bind state
+
+extern "C" int hexdyn_bind_state(HexDynHandle* h, const HexDynFields* fields, void* stream) {
+  if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
+  HexCtx& c = h->ctx;
+  if (!fields) {
+    if (h->bound) {
+      if (c.parity == 0) return fail(HEXDYN_E_STATE, "the current state is in the bound buffers; step once more "
+                                     "(or copy it) before unbinding");
+      c.in = h->own_in;
+      c.side_in = h->own_side_in;
+      h->bound = false;
+    }
+  } else {
+    for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i) {
+      const float* p = fields->field[i];
+      if (!p && !(i == HEXDYN_SCALARS && c.n_scalars == 0))
+        return fail(HEXDYN_E_ARG, "bound field %d is NULL", i);
+      if ((uintptr_t)p & 15u)
+        return fail(HEXDYN_E_ARG, "bound field %d is not 16-byte aligned (the kernels move four levels per "
+                    "128-bit access)", i);
+      if (p && p == field_ptr(c.out, c.side_out, i))
+        return fail(HEXDYN_E_ARG, "bound field %d is the handle's own output buffer", i);
+    }
+    if (!h->bound) {
+      h->own_in = c.in;
+      h->own_side_in = c.side_in;
+    }
+    c.in = HexState{fields->field[HEXDYN_RHO], fields->field[HEXDYN_RHO_THETA], fields->field[HEXDYN_RHO_U],
+                    fields->field[HEXDYN_RHO_W], fields->field[HEXDYN_SCALARS]};
+    c.side_in = HexSide{fields->field[HEXDYN_THETA_M], fields->field[HEXDYN_EXNER], fields->field[HEXDYN_RHO_P],
+                        fields->field[HEXDYN_RHO_THETA_P], fields->field[HEXDYN_PRESSURE_P], fields->field[HEXDYN_U],
+                        fields->field[HEXDYN_W]};
+    c.parity = 0;
+    h->bound = true;
+    for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f) h->have_state[f] = true;
+  }
+  // captured graphs hold the old buffer addresses
+  if (c.graph_exec[0] || c.graph_exec[1]) return hexdyn_capture_graph(h, stream);
+  return HEXDYN_OK;
+}
+
 // ------------------------------------------------------------ no-alloc step
 // hexdyn_step_noalloc: the large step with its scratch in a file-scope device
 // array instead of the handle's workspace (declaration and contract in
@@ -1437,6 +1484,10 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   HexSide d_in, d_out;
   if (!fields_of(in, src.n_scalars, s_in, d_in) || !fields_of(out, src.n_scalars, s_out, d_out))
     return fail(HEXDYN_E_ARG, "every state and sidecar field needs a device pointer");
+  for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i)
+    if (((uintptr_t)in->field[i] | (uintptr_t)out->field[i]) & 15u)
+      return fail(HEXDYN_E_ARG, "field %d is not 16-byte aligned (the kernels move four levels per 128-bit access)",
+                  i);
   for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i)
     for (int j = 0; j < HEXDYN_NUM_FIELDS; ++j)
       if (in->field[i] && in->field[i] == out->field[j])

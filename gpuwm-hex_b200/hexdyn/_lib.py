@@ -97,6 +97,7 @@ EXPORTS = {
                                           C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hexdyn_total_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hexdyn_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
+    "hexdyn_bind_state": (C.c_int, [C.c_void_p, C.POINTER(HexDynFields), C.c_void_p]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -249,6 +249,21 @@ class HexDycoreDriver:
             out[name] = {"us": {64: float(t64), 128: float(t128), 256: float(t256)}, "threads": int(chosen)}
         return out
 
+    def bind_state(self, tensors: dict | None) -> None:
+        """Step from caller-owned CUDA tensors (padded layout, one per field
+        name of ``hexdyn._lib.FIELDS``) without copying; ``None`` unbinds.
+        The step alternates between these and the library's own buffers."""
+        if tensors is None:
+            _lib.check(self._lib.hexdyn_bind_state(self._handle, None, self._stream_handle()))
+            self._keep.pop("_bound", None)
+            return
+        f = _lib.HexDynFields()
+        for name, i in _lib.FIELDS.items():
+            t = tensors.get(name)
+            f.field[i] = None if t is None else int(t.data_ptr())
+        _lib.check(self._lib.hexdyn_bind_state(self._handle, C.byref(f), self._stream_handle()))
+        self._keep["_bound"] = dict(tensors)
+
     # -------------------------------------------------------------- steps
     def step_async(self, nsteps: int = 1) -> None:
         _lib.check(self._lib.hexdyn_step_async(self._handle, self._stream_handle(), int(nsteps)))

@@ -190,6 +190,17 @@ typedef struct HexDynFields {
   float* field[HEXDYN_NUM_FIELDS];
 } HexDynFields;
 
+/* Bind caller-owned device buffers (padded layout, 16-byte aligned, every
+ * field; replaces the reference's DeviceAtmosphere handed to the driver,
+ * hexcore/cuda_driver.py:5419) as the current state
+ * and sidecar; the handle steps from them without a copy.  Each step
+ * publishes the new state in the other buffer set, as the reference does, so
+ * after an odd number of steps the state is in the library's own buffers and
+ * after an even number back in the bound ones (hexdyn_device_field always
+ * points at the current state).  fields == NULL unbinds (when the current
+ * state is in the library's buffers).  Captured graphs are captured again. */
+int hexdyn_bind_state(HexDynHandle* h, const HexDynFields* fields, void* stream);
+
 /* No counterpart in the reference: one large step that allocates nothing.
  * For callers that cannot call cudaMalloc when they step -- code running
  * while its own stream is being captured into a CUDA graph (an allocation

@@ -6,7 +6,7 @@ by ``hexdyn.case`` and stores inputs and outputs as ``.npz`` fixtures.  It
 needs the reference checkout (default ``/root/reference``) and therefore runs
 only where that exists; the fixtures it writes are what the tests read.
 
-Harness (SURVEY section 8c): a two-class ``netCDF4`` stub and a ``gpuwm``
+Harness: a two-class ``netCDF4`` stub and a ``gpuwm``
 stub are put on ``sys.path`` (the reference imports them only for file I/O
 and LES route checks); the advection coefficients, vertical grid and terrain
 metrics the reference would take from its Rust engines are supplied by the

@@ -28,6 +28,7 @@
 // Every wait on an mbarrier is bounded: past the limit the kernel records
 // an error in *err, stops issuing work, waits (bounded again) for its own
 // MMAs, frees its tensor memory and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -119,13 +120,17 @@ __device__ __forceinline__ float tanh_hw(float x) {
   return y;
 }
 constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2/pi)
-constexpr float GELU_A = 0.044715f;
+constexpr float GELU_CA = 0.7978845608028654f * 0.044715f;
+// tanh argument sqrt(2/pi) (x + 0.044715 x^3) written as x (C + C A x^2)
 __device__ __forceinline__ float gelu(float x) {
-  return 0.5f * x * (1.0f + tanh_hw(GELU_C * (x + GELU_A * x * x * x)));
+  const float hx = 0.5f * x;
+  return __fmaf_rn(hx, tanh_hw(x * __fmaf_rn(GELU_CA, x * x, GELU_C)), hx);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float t = tanh_hw(GELU_C * (x + GELU_A * x * x * x));
-  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_C * (1.0f + 3.0f * GELU_A * x * x);
+  const float x2 = x * x;
+  const float t = tanh_hw(x * __fmaf_rn(GELU_CA, x2, GELU_C));
+  // 0.5 (1 + t) + 0.5 x (1 - t^2) (C + 3 C A x^2)
+  return __fmaf_rn(0.5f * x * __fmaf_rn(-t, t, 1.0f), __fmaf_rn(3.0f * GELU_CA, x2, GELU_C), __fmaf_rn(0.5f, t, 0.5f));
 }
 
 // Asynchronous copy of a rows x 64 slab (K-contiguous rows of length ld)
@@ -161,6 +166,59 @@ struct Gemm {
   float* Cf;
   int* err;
 };
+
+// Epilogue of 8 accumulator columns of one row: bias, then the selected
+// epilogue, stores of C / C^T / Z / Cf (shared by both GEMM kernels).
+__device__ __forceinline__ void epilogue8(const Gemm& p, int row, int col, float* v) {
+  if (p.bias) {
+    // the same 8 bias words for every lane of the warp: two broadcast 128-bit loads
+    const float4 b0 = __ldg(reinterpret_cast<const float4*>(p.bias + col));
+    const float4 b1 = __ldg(reinterpret_cast<const float4*>(p.bias + col + 4));
+    v[0] += b0.x;
+    v[1] += b0.y;
+    v[2] += b0.z;
+    v[3] += b0.w;
+    v[4] += b1.x;
+    v[5] += b1.y;
+    v[6] += b1.z;
+    v[7] += b1.w;
+  }
+  if (p.epilogue == HEXMLP_EPI_GELU) {
+    __nv_bfloat16 z[8], h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      z[i] = __float2bfloat16_rn(v[i]);
+      h[i] = __float2bfloat16_rn(gelu(v[i]));
+    }
+    if (p.Z) *reinterpret_cast<uint4*>(p.Z + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(z);
+    if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(h);
+    if (p.Ct) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = h[i];
+    }
+  } else if (p.epilogue == HEXMLP_EPI_GELU_GRAD) {
+    __nv_bfloat16 d[8];
+    const uint4 zr = *reinterpret_cast<const uint4*>(p.Zin + (size_t)row * p.N + col);
+    const __nv_bfloat16* zz = reinterpret_cast<const __nv_bfloat16*>(&zr);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) d[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zz[i])));
+    if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(d);
+    if (p.Ct) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = d[i];
+    }
+  } else {
+    float4* dst = reinterpret_cast<float4*>(p.Cf + (size_t)row * p.N + col);
+    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+    if (p.C) {
+      __nv_bfloat16 b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) b[i] = __float2bfloat16_rn(v[i]);
+      *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(b);
+    }
+  }
+}
 
 __global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -257,48 +315,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
       for (int g8 = 0; g8 < 4; ++g8) {
       float* v = v32 + 8 * g8;
       const int col = n0 + c32 + 8 * g8;
-      if (p.bias) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] += p.bias[col + i];
-      }
-      if (p.epilogue == HEXMLP_EPI_GELU) {
-        // Z (pre-activation) for the backward pass, H = GELU(Z) and H^T
-        __nv_bfloat16 z[8], h[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          z[i] = __float2bfloat16_rn(v[i]);
-          h[i] = __float2bfloat16_rn(gelu(v[i]));
-        }
-        if (p.Z) *reinterpret_cast<uint4*>(p.Z + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(z);
-        if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(h);
-        if (p.Ct) {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = h[i];
-        }
-      } else if (p.epilogue == HEXMLP_EPI_GELU_GRAD) {
-        // dZ = (dH) * GELU'(Z) with Z of this layer's forward pass
-        __nv_bfloat16 d[8];
-        const uint4 zr = *reinterpret_cast<const uint4*>(p.Zin + (size_t)row * p.N + col);
-        const __nv_bfloat16* zz = reinterpret_cast<const __nv_bfloat16*>(&zr);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) d[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zz[i])));
-        if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(d);
-        if (p.Ct) {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = d[i];
-        }
-      } else {
-        // FP32 result (output layer, weight gradient)
-        float4* dst = reinterpret_cast<float4*>(p.Cf + (size_t)row * p.N + col);
-        dst[0] = make_float4(v[0], v[1], v[2], v[3]);
-        dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-        if (p.C) {
-          __nv_bfloat16 b[8];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) b[i] = __float2bfloat16_rn(v[i]);
-          *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(b);
-        }
-      }
+      epilogue8(p, row, col, v);
       }
     }
   } else if (threadIdx.x == 0 && issued > 0) {
@@ -311,6 +328,180 @@ __global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent warp-specialised GEMM.  One CTA per SM loops over output tiles
+// (128 x BN, n fastest so that consecutive tiles reuse the same A rows from
+// L2).  Warp 0 (one lane) loads 64-element K slabs of A and B with TMA
+// (128-byte swizzle, completion counted in bytes on the stage's "full"
+// mbarrier) into an NS-stage ring; warp 1 (one lane) issues four K=16
+// tcgen05.mma per slab into one of two tensor-memory accumulators and
+// commits each slab to the stage's "empty" mbarrier and each finished tile
+// to the accumulator's "full" mbarrier; warps 2..9 drain the other
+// accumulator (warp w reads lanes 32(w%4).. and one half of the columns),
+// apply the epilogue and store, then release the accumulator.  The
+// epilogue of tile i thus overlaps the loads and MMAs of tile i+1.  Every
+// wait is bounded; a role that gives up raises the CTA's abort word and
+// all roles stop.
+constexpr int WS_THREADS = 320;
+constexpr int WS_STAGES = 4;
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+// K-major, 128-byte swizzle: 8-row groups 1024 bytes apart (stride offset),
+// leading offset unused (1), layout type 2.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+    k_gemm_ws(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Gemm p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // stage buffers on a 1024-byte boundary (the swizzle atom)
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE = A_BYTES + B_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + WS_STAGES * STAGE);
+  uint64_t* empty = full + WS_STAGES;
+  uint64_t* acc_full = empty + WS_STAGES;
+  uint64_t* acc_empty = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  volatile int* abort_word = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_n = p.N / BN, tiles = (p.M / BM) * n_n, nk = p.K / BK;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < WS_STAGES; ++i) {
+      mbar_init(smem_u32(&full[i]), 1);
+      mbar_init(smem_u32(&empty[i]), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_u32(&acc_full[i]), 1);
+      mbar_init(smem_u32(&acc_empty[i]), 8);  // one arrival per epilogue warp
+    }
+    *abort_word = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // TMA producer
+    if (lane == 0) {
+      int it = 0;
+      for (int t = blockIdx.x; t < tiles && !*abort_word; t += gridDim.x) {
+        const int m0 = (t / n_n) * BM, n0 = (t % n_n) * BN;
+        for (int kt = 0; kt < nk; ++kt, ++it) {
+          const int s = it % WS_STAGES;
+          if (!mbar_wait(smem_u32(&empty[s]), ((it / WS_STAGES) & 1) ^ 1)) {
+            *abort_word = 1;
+            break;
+          }
+          uint8_t* a = smem + s * STAGE;
+          mbar_expect_tx(smem_u32(&full[s]), STAGE);
+          tma_load_2d(smem_u32(a), &tmA, kt * BK, m0, smem_u32(&full[s]));
+          tma_load_2d(smem_u32(a + A_BYTES), &tmB, kt * BK, n0, smem_u32(&full[s]));
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc(BM, BN);
+      int it = 0, tc = 0;
+      for (int t = blockIdx.x; t < tiles && !*abort_word; t += gridDim.x, ++tc) {
+        const int b = tc & 1;
+        if (!mbar_wait(smem_u32(&acc_empty[b]), ((tc >> 1) & 1) ^ 1)) {
+          *abort_word = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * BN);
+        for (int kt = 0; kt < nk; ++kt, ++it) {
+          const int s = it % WS_STAGES;
+          if (!mbar_wait(smem_u32(&full[s]), (it / WS_STAGES) & 1)) {
+            *abort_word = 1;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(smem + s * STAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+          for (int j = 0; j < BK / 16; ++j)
+            mma_bf16(acc, umma_desc_sw128(a0 + 32 * j), umma_desc_sw128(b0 + 32 * j), idesc,
+                     (kt > 0 || j > 0) ? 1u : 0u);
+          mma_commit(smem_u32(&empty[s]));
+        }
+        if (*abort_word) break;
+        mma_commit(smem_u32(&acc_full[b]));
+      }
+    }
+  } else {
+    // epilogue warps 2..9: lane quarter warp % 4, column half (warp - 2) / 4
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    int tc = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tc) {
+      const int b = tc & 1;
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(smem_u32(&acc_full[b]), (tc >> 1) & 1);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) {
+        if (lane == 0) *abort_word = 1;
+        break;
+      }
+      if (*abort_word) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int m0 = (t / n_n) * BM, n0 = (t % n_n) * BN;
+      const int row = m0 + quarter * 32 + lane;
+      const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN);
+      for (int c32 = half * (BN / 2); c32 < (half + 1) * (BN / 2); c32 += 32) {
+        float v32[32];
+        tmem_ld32(base + (uint32_t)c32, v32);
+#pragma unroll
+        for (int g8 = 0; g8 < 4; ++g8) epilogue8(p, row, n0 + c32 + 8 * g8, v32 + 8 * g8);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+    }
+  }
+  __syncthreads();
+  if (*abort_word) {
+    if (threadIdx.x == 0) atomicOr(p.err, 1);
+    // bounded wait for the last accumulator commit of each buffer still in flight
+    if (threadIdx.x == 32)
+      for (int b = 0; b < 2; ++b) mbar_wait(smem_u32(&acc_full[b]), 0);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
   }
 }
 
@@ -410,6 +601,62 @@ size_t hexmlp_gemm_smem_bytes(int bn) { return (size_t)NSTAGE * (BM + bn) * BK *
 int hexmlp_gemm_tile_rows(void) { return BM; }
 int hexmlp_gemm_tile_k(void) { return BK; }
 
+}  // extern "C"
+
+namespace {
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiled)f;
+  }
+  return fn;
+}
+
+// [rows][K] bf16 row-major, boxes of 64 K-elements x box_rows rows, 128-byte swizzle
+bool make_map(CUtensorMap* m, const void* base, int rows, int K, int box_rows) {
+  EncodeTiled fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN>
+size_t ws_smem_bytes() {
+  return (size_t)WS_STAGES * (BM + BN) * BK * 2 + 1024 + 256;
+}
+
+template <int BN>
+int launch_ws(const Gemm& g, cudaStream_t st) {
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, g.A, g.M, g.K, BM) || !make_map(&tb, g.B, g.N, g.K, BN)) return HEXMLP_E_ARG;
+  static int sms = 0;
+  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const size_t smem = ws_smem_bytes<BN>();
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_ws<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return (int)e;
+  const int tiles = (g.M / BM) * (g.N / BN);
+  k_gemm_ws<BN><<<tiles < sms ? tiles : sms, WS_THREADS, smem, st>>>(ta, tb, g);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
 int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
   if (!p || !p->A || !p->B || !p->err) return HEXMLP_E_ARG;
   if (p->M <= 0 || p->N <= 0 || p->K <= 0 || p->M % BM || p->K % BK) return HEXMLP_E_ARG;
@@ -419,7 +666,7 @@ int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
   if (p->epilogue < HEXMLP_EPI_F32 || p->epilogue > HEXMLP_EPI_GELU_GRAD) return HEXMLP_E_ARG;
   // 16-byte alignment of every row: K and N multiples of 8 hold by the checks
   // above; the base pointers must be 16-byte aligned
-  const void* ptrs[] = {p->A, p->B, p->C, p->Z, p->Zin, p->Cf};
+  const void* ptrs[] = {p->A, p->B, p->C, p->Z, p->Zin, p->Cf, p->bias};
   for (const void* q : ptrs)
     if (q && ((uintptr_t)q & 15u)) return HEXMLP_E_ARG;
   const size_t smem = hexmlp_gemm_smem_bytes(p->bn);
@@ -427,6 +674,9 @@ int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
   if (e != cudaSuccess) return (int)e;
   const Gemm g{(const bf16*)p->A, (const bf16*)p->B, p->M, p->N, p->K, p->bn, p->epilogue, p->bias, (bf16*)p->C,
                (bf16*)p->Ct, (bf16*)p->Z, (const bf16*)p->Zin, p->Cf, p->err};
+  if (p->kernel == HEXMLP_GEMM_PERSISTENT)
+    return p->bn == 256 ? launch_ws<256>(g, (cudaStream_t)stream) : launch_ws<128>(g, (cudaStream_t)stream);
+  if (p->kernel != HEXMLP_GEMM_STAGED) return HEXMLP_E_ARG;
   dim3 grid(p->M / BM, p->N / p->bn);
   k_gemm_bf16<<<grid, THREADS, smem, (cudaStream_t)stream>>>(g);
   return (int)cudaGetLastError();

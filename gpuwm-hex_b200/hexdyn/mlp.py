@@ -28,7 +28,10 @@ class HexMlpGemm(C.Structure):
     _fields_ = [("A", C.c_void_p), ("B", C.c_void_p), ("M", C.c_int32), ("N", C.c_int32), ("K", C.c_int32),
                 ("bn", C.c_int32), ("epilogue", C.c_int32), ("bias", C.c_void_p), ("C", C.c_void_p),
                 ("Ct", C.c_void_p), ("Z", C.c_void_p), ("Zin", C.c_void_p), ("Cf", C.c_void_p),
-                ("err", C.c_void_p)]
+                ("err", C.c_void_p), ("kernel", C.c_int32)]
+
+
+GEMM_PERSISTENT, GEMM_STAGED = 0, 1
 
 
 MLP_EXPORTS = {
@@ -78,9 +81,10 @@ def round_up(x: int, m: int) -> int:
 
 
 def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=None, Zin=None, Cf=None, err=None,
-         bn: int = 128):
+         bn: int | None = None, kernel: int = GEMM_PERSISTENT):
     """C = A . B^T on the tensor cores (see include/hexmlp.h).  ``bn``: the
-    output tile width, 128 (two CTAs per SM, the default) or 256."""
+    output tile width, 128 or 256 (default: 256 where N allows it for the
+    persistent kernel, 128 for the staged one)."""
     import torch
 
     M, K = A.shape
@@ -89,8 +93,10 @@ def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=Non
     assert A.is_contiguous() and B.is_contiguous()
     if err is None:
         err = torch.zeros(1, dtype=torch.int32, device=A.device)
+    if bn is None:
+        bn = 256 if (kernel == GEMM_PERSISTENT and N % 256 == 0) else 128
     p = HexMlpGemm(_ptr(A), _ptr(B), M, N, K, bn, epilogue, _ptr(bias), _ptr(C_out), _ptr(Ct), _ptr(Z), _ptr(Zin),
-                   _ptr(Cf), _ptr(err))
+                   _ptr(Cf), _ptr(err), kernel)
     _check(load().hexmlp_gemm(C.byref(p), _stream()), f"hexmlp_gemm {M}x{N}x{K}")
     return err
 
@@ -176,8 +182,9 @@ class TensorCoreMLP:
         a = X
         for i in range(self.depth):
             lay = self.layers[i]
+            # the pre-activations and transposed activations are kept for the backward pass only
             gemm(a, lay.wb, epilogue=EPI_GELU, bias=lay.b, C_out=ws["H"][i], Ct=ws["Ht"][i] if keep else None,
-                 Z=ws["Z"][i], err=self.err)
+                 Z=ws["Z"][i] if keep else None, err=self.err)
             a = ws["H"][i]
         last = self.layers[-1]
         gemm(a, last.wb, epilogue=EPI_F32, bias=last.b, Cf=ws["Y"], err=self.err)

@@ -44,7 +44,14 @@ typedef struct HexMlpGemm {
   const void* Zin;     /* bf16 [M][N] (HEXMLP_EPI_GELU_GRAD) */
   float* Cf;           /* float [M][N] (HEXMLP_EPI_F32) */
   int* err;            /* device int */
+  int32_t kernel;      /* HEXMLP_GEMM_PERSISTENT (default) or HEXMLP_GEMM_STAGED */
 } HexMlpGemm;
+
+/* GEMM kernels: persistent and warp-specialised (TMA loads, one MMA thread,
+ * epilogue warps on a double-buffered tensor-memory accumulator), or one CTA
+ * per tile with cp.async staging. */
+#define HEXMLP_GEMM_PERSISTENT 0
+#define HEXMLP_GEMM_STAGED 1
 
 int hexmlp_gemm(const HexMlpGemm* p, void* stream);
 size_t hexmlp_gemm_smem_bytes(int bn);

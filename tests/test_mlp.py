@@ -54,20 +54,20 @@ def _bf(x):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N,bn", [(384, 128), (512, 256)])
-def test_gemm_epilogues_match_float64(N, bn):
+@pytest.mark.parametrize("N,bn,kernel", [(384, 128, 0), (512, 256, 0), (384, 128, 1), (512, 256, 1)])
+def test_gemm_epilogues_match_float64(N, bn, kernel):
     from hexdyn import mlp
 
     assert torch.cuda.is_available()
     rng = np.random.default_rng(N)
-    M, K = 256, 192
+    M, K = 640, 192  # five row tiles: the persistent kernel loops over several tiles per CTA
     A = om.bf16(rng.standard_normal((M, K)).astype(np.float32))
     B = om.bf16(rng.standard_normal((N, K)).astype(np.float32) * 0.1)
     bias = rng.standard_normal(N).astype(np.float32)
     ref = A.astype(np.float64) @ B.astype(np.float64).T
     At, Bt = _bf(A), _bf(B)
     Cf = torch.empty(M, N, dtype=torch.float32, device="cuda")
-    err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf, bn=bn)
+    err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf, bn=bn, kernel=kernel)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     np.testing.assert_allclose(Cf.cpu().numpy(), ref, rtol=0, atol=1e-4 * np.abs(ref).max())
@@ -75,7 +75,7 @@ def test_gemm_epilogues_match_float64(N, bn):
     H = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
     Ht = torch.empty(N, M, dtype=torch.bfloat16, device="cuda")
     Z = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
-    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU, bias=torch.from_numpy(bias).cuda(), C_out=H, Ct=Ht, Z=Z, err=err, bn=bn)
+    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU, bias=torch.from_numpy(bias).cuda(), C_out=H, Ct=Ht, Z=Z, err=err, bn=bn, kernel=kernel)
     z = ref + bias
     np.testing.assert_allclose(Z.float().cpu().numpy(), z, rtol=1e-2, atol=1e-2)
     h = om.gelu(z)
@@ -84,7 +84,7 @@ def test_gemm_epilogues_match_float64(N, bn):
     # GELU' epilogue on a given Z
     D = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
     Dt = torch.empty(N, M, dtype=torch.bfloat16, device="cuda")
-    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU_GRAD, C_out=D, Ct=Dt, Zin=Z, err=err, bn=bn)
+    mlp.gemm(At, Bt, epilogue=mlp.EPI_GELU_GRAD, C_out=D, Ct=Dt, Zin=Z, err=err, bn=bn, kernel=kernel)
     want = ref * om.gelu_grad(Z.float().cpu().numpy())
     np.testing.assert_allclose(D.float().cpu().numpy(), want, rtol=1e-2, atol=1e-2 * np.abs(want).max())
     np.testing.assert_array_equal(Dt.float().cpu().numpy(), D.float().cpu().numpy().T)

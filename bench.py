@@ -94,7 +94,7 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_ac_cell_first": el + 12 * cl + 7 * ci + conn_c,        # old perturbations are zero
         "k_ac_cell": el + 16 * cl + 9 * ci + conn_c,
         "k_recover_edge": 7 * el + 3 * cl + conn_e,
-        "k_recover_cell": el + 15 * cl + 7 * ci + zb + conn_c,
+        "k_recover_cell": el + 16 * cl + 7 * ci + zb + conn_c,       # + the next stage's hdiv
         "k_tr_edge": (tcl + tel) + el + adv,
         "k_tr_edge_mono": (tcl + tel) + el + adv,
         "k_tr_std": 3 * tcl + tel + 2 * cl + el + ci + conn_c,

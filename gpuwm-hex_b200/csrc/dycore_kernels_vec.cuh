@@ -619,7 +619,7 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
                                 const float* __restrict__ rw_p, const float* __restrict__ ww_avg,
                                 const float* __restrict__ ru_new, HexState out, HexSide side,
                                 float* __restrict__ flux_w, int flux_mode, float inv_steps, float inv_splits,
-                                int* flag) {
+                                int* flag, float* __restrict__ hdiv_next) {
   HEX_VEC_PARALLEL(g.nC)
   const int c = ent, S = g.S, L = g.L;
   const int ii = c * S + k0;
@@ -688,10 +688,16 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
     acc[j] = 0.0f;
     if (k >= 1 && k < L) acc[j] = rwv.a[j] / (g.fzm[k] * zzw(j) + g.fzp[k] * zzw(j - 1));
   }
+  // the next stage's mass-flux divergence of ru_new (mass_flux_div4, the
+  // same operands in the same order) accumulates in the same edge loop
+  V4 hd = v4zero();
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float sign = g.csign[c * g.maxE + s];
     const V4 r = ld4(ru_new + e * S + k0);
+    const float sd = sign * g.dv[e];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) hd.a[j] = hd.a[j] + sd * r.a[j];
     const float rm = k0 > 0 ? ru_new[e * S + k0 - 1] : 0.0f;
     const int zi = (c * g.maxE + s) * S + k0;
     const V4 zb = ld4(g.zb + zi), zb3 = ld4(g.zb3 + zi);
@@ -723,6 +729,12 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
     wv.a[j] = wk;
   }
   st4m(side.w + ii, wv, k0, 0, g.L + 1);
+  {
+    const float ia = g.inv_area[c];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) hd.a[j] = hd.a[j] * ia;
+    st4m(hdiv_next + ii, hd, k0, 0, g.L);
+  }
   if (flux_mode & 4) {
     const V4 av = ld4(ww_avg + ii);
     const V4 old = (flux_mode & 1) ? v4zero() : ld4rw(flux_w + ii);

@@ -156,7 +156,9 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
       }
-      LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
+      // the mass-flux divergence of cur->rho_u: computed by the previous
+      // stage's recovery, except for the first stage of the step
+      if (sub == 0 && si == 0) LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
       LPS(L, g.nE, 1, edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
            w.edge_theta, w.edge_w);
       LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
@@ -206,7 +208,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       LPS(L, g.nC, 1, recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
            (const float*)s_in->rtheta_p, (const float*)saved->rho_w, (const float*)w.rho_pp, rtpp_final,
            (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
-           inv_splits, w.flag);
+           inv_splits, w.flag, w.hdiv);
       diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
       cur = &o;
       cs = &so;

@@ -17,8 +17,24 @@ SIDE = ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
 
 
 def load_golden(name: str) -> dict:
+    """A fixture; configuration variants carry only outputs and take their
+    inputs from the base case they name."""
     with np.load(GOLDEN / f"step_{name}.npz", allow_pickle=False) as z:
-        return {k: z[k] for k in z.files}
+        fx = {k: z[k] for k in z.files}
+    if "base" in fx:
+        base = load_golden(str(fx["base"]))
+        fx.update({k: v for k, v in base.items() if k.startswith("in.")})
+    return fx
+
+
+def golden_config(fx: dict) -> dict:
+    """The configuration a fixture was made with (defaults of the base cases)."""
+    return {"dt": float(fx["config.dt"]), "n_sub_steps": int(fx["config.n_sub_steps"]),
+            "monotonic": bool(int(fx.get("config.monotonic", 1))),
+            "apvm_upwinding": float(fx.get("config.apvm_upwinding", 0.5))}
+
+
+VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1)]
 
 
 def inputs(fx: dict) -> dict:

@@ -15,7 +15,7 @@ case builder.  The ``native`` fixture wraps the driver so that
 carried scalar (``hexcore/regional_v841.py:1180``), which is what native MPAS
 and the reference's CUDA driver apply with physics off.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py [/path/to/reference [fixture names ...]]
 """
 
 from __future__ import annotations
@@ -40,6 +40,15 @@ CASES = {
     "l3_L20": (3, 20, 0, 1800.0, 2, 1, False),
 }
 
+# Configuration variants on the inputs of a base case (outputs only; the
+# fixture names its base): name -> (base, sub steps, monotonic, apvm, steps)
+VARIANTS = {
+    "l2_L12_sub1": ("l2_L12", 1, True, 0.5, 2),     # one acoustic substep per stage
+    "l2_L12_sub4": ("l2_L12", 4, True, 0.5, 2),     # (1, 2, 4) substeps
+    "l2_L12_nomono": ("l2_L12", 2, False, 0.5, 2),  # standard RK3 transport
+    "l2_L12_noapvm": ("l2_L12", 2, True, 0.0, 1),   # no APVM upwinding
+}
+
 
 def _stubs() -> str:
     d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
@@ -54,7 +63,7 @@ def _stubs() -> str:
     return str(d)
 
 
-def main(reference_root: str = "/root/reference") -> None:
+def main(reference_root: str = "/root/reference", *only: str) -> None:
     sys.path.insert(0, _stubs())
     sys.path.insert(0, str(Path(reference_root) / "tree" / "src"))
     from hexcore.config_v841 import V841DryDycoreConfig
@@ -77,7 +86,23 @@ def main(reference_root: str = "/root/reference") -> None:
             kw.update(moist_cqu=cqu, moist_cqw=cqw, moist_qtot=qtot)
             return super()._advance_dynamics_subcycle(state, **kw)
 
+    def run(cls, mesh, vg, ref, cfg, ac, tm, wp, case, nsteps, label, out):
+        drv = cls(mesh, vg, ref, cfg, advection_coefficients=ac, terrain_metrics=tm, reference_wind_profiles=wp)
+        state = PrognosticState(case.rho.copy(), case.rho_theta.copy(), case.rho_u.copy(), case.rho_w.copy(),
+                                case.scalars.copy(), 0.0)
+        side = None
+        for step in range(1, nsteps + 1):
+            res = drv.step(state, saved_diagnostics=side)
+            state, side = res.state, res.saved_diagnostics
+            for k in ("rho", "rho_theta", "rho_u", "rho_w", "scalars"):
+                out[f"{label}.step{step}.{k}"] = np.asarray(getattr(state, k))
+            for k in ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
+                      "pressure_perturbation", "normal_velocity", "vertical_velocity"):
+                out[f"{label}.step{step}.side.{k}"] = np.asarray(getattr(side, k))
+
     for name, (level, nlev, ncond, dt, nsub, nsteps, native) in CASES.items():
+        if only and name not in only and not any(v[0] == name for k, v in VARIANTS.items() if k in only):
+            continue
         t0 = time.time()
         mesh = build_mesh(level, lloyd=20, seed=0)
         case = build_case(mesh, n_levels=nlev, seed=0, n_condensates=ncond)
@@ -94,24 +119,27 @@ def main(reference_root: str = "/root/reference") -> None:
         out = {f"in.{k}": v for k, v in case_arrays(case).items()}
         out["config.dt"] = dt
         out["config.n_sub_steps"] = nsub
-        runs = [("dry", DryDycoreDriver)] + ([("native", NativeMoistDriver)] if native else [])
-        for label, cls in runs:
-            drv = cls(mesh, vg, ref, cfg, advection_coefficients=ac, terrain_metrics=tm,
-                      reference_wind_profiles=wp)
-            state = PrognosticState(case.rho.copy(), case.rho_theta.copy(), case.rho_u.copy(),
-                                    case.rho_w.copy(), case.scalars.copy(), 0.0)
-            side = None
-            for step in range(1, (nsteps if label == "dry" else 1) + 1):
-                res = drv.step(state, saved_diagnostics=side)
-                state, side = res.state, res.saved_diagnostics
-                for k in ("rho", "rho_theta", "rho_u", "rho_w", "scalars"):
-                    out[f"{label}.step{step}.{k}"] = np.asarray(getattr(state, k))
-                for k in ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
-                          "pressure_perturbation", "normal_velocity", "vertical_velocity"):
-                    out[f"{label}.step{step}.side.{k}"] = np.asarray(getattr(side, k))
-        path = HERE / f"step_{name}.npz"
-        np.savez_compressed(path, **out)
-        print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
+        if not only or name in only:
+            runs = [("dry", DryDycoreDriver)] + ([("native", NativeMoistDriver)] if native else [])
+            for label, cls in runs:
+                run(cls, mesh, vg, ref, cfg, ac, tm, wp, case, nsteps if label == "dry" else 1, label, out)
+            path = HERE / f"step_{name}.npz"
+            np.savez_compressed(path, **out)
+            print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
+        for vname, (base, vsub, mono, apvm, vsteps) in VARIANTS.items():
+            if base != name or (only and vname not in only):
+                continue
+            t0 = time.time()
+            vcfg = V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=vsub, config_dynamics_split_steps=3,
+                                       config_split_dynamics_transport=True, config_monotonic=mono,
+                                       config_positive_definite=False, config_coef_3rd_order=0.25,
+                                       config_apvm_upwinding=apvm)
+            vout = {"base": np.array(base), "config.dt": dt, "config.n_sub_steps": vsub,
+                    "config.monotonic": int(mono), "config.apvm_upwinding": apvm}
+            run(DryDycoreDriver, mesh, vg, ref, vcfg, ac, tm, wp, case, vsteps, "dry", vout)
+            path = HERE / f"step_{vname}.npz"
+            np.savez_compressed(path, **vout)
+            print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
 
 
 if __name__ == "__main__":

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import hexdyn
-from fixtures import SIDE, STATE, case_from_arrays, differing_words, inputs, load_golden
+from fixtures import SIDE, STATE, VARIANTS, case_from_arrays, differing_words, golden_config, inputs, load_golden
 from hexdyn.case import build_case, case_arrays
 from hexdyn.config import DycoreConfig
 from hexdyn.mesh import build_mesh
@@ -44,6 +44,26 @@ def test_strict_step_matches_reference_outputs(name, label, steps):
             assert differing_words(getattr(res.state, k), fx[f"{label}.step{step}.{k}"]) == 0, (step, k)
         for k in SIDE:
             assert differing_words(getattr(res.saved_diagnostics, k), fx[f"{label}.step{step}.side.{k}"]) == 0, (step, k)
+    drv.close()
+
+
+@pytest.mark.parametrize("name,steps", VARIANTS)
+def test_strict_step_matches_reference_variants(name, steps):
+    """One and four acoustic substeps, standard RK3 transport, no APVM: the
+    CUDA step against the reference run with that configuration."""
+    fx = load_golden(name)
+    c = golden_config(fx)
+    cfg = DycoreConfig(config_dt=c["dt"], config_number_of_sub_steps=c["n_sub_steps"],
+                       config_monotonic=c["monotonic"], config_apvm_upwinding=c["apvm_upwinding"],
+                       moist_coefficients="dry")
+    drv = hexdyn.from_case(case_from_arrays(inputs(fx)), cfg, capture_graph=True)
+    for step in range(1, steps + 1):
+        res = drv.step()
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), fx[f"dry.step{step}.{k}"]) == 0, (name, step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), fx[f"dry.step{step}.side.{k}"]) == 0, \
+                (name, step, k)
     drv.close()
 
 

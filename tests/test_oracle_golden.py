@@ -9,7 +9,7 @@ The oracle must reproduce every output word.
 import numpy as np
 import pytest
 
-from fixtures import SIDE, STATE, differing_words, inputs, load_golden
+from fixtures import SIDE, STATE, VARIANTS, differing_words, golden_config, inputs, load_golden
 from oracle.dycore import OracleConfig, OracleDycore, State
 
 
@@ -27,6 +27,25 @@ def test_oracle_matches_reference_bitwise(name, label, steps):
             assert differing_words(getattr(state, k), fx[f"{label}.step{step}.{k}"]) == 0, (label, step, k)
         for k in SIDE:
             assert differing_words(getattr(side, k), fx[f"{label}.step{step}.side.{k}"]) == 0, (label, step, k)
+
+
+@pytest.mark.parametrize("name,steps", VARIANTS)
+def test_oracle_matches_reference_variants(name, steps):
+    """Configuration variants (one and four acoustic substeps, standard RK3
+    transport, no APVM) against the reference run with that configuration."""
+    fx = load_golden(name)
+    c = golden_config(fx)
+    arr = inputs(fx)
+    orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["n_sub_steps"], monotonic=c["monotonic"],
+                                         apvm_upwinding=c["apvm_upwinding"], moist="dry"))
+    state = State(*(arr[k].copy() for k in STATE))
+    side = None
+    for step in range(1, steps + 1):
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(state, k), fx[f"dry.step{step}.{k}"]) == 0, (name, step, k)
+        for k in SIDE:
+            assert differing_words(getattr(side, k), fx[f"dry.step{step}.side.{k}"]) == 0, (name, step, k)
 
 
 def test_native_moist_coefficients_change_the_step():

@@ -24,6 +24,8 @@ def load_golden(name: str) -> dict:
     if "base" in fx:
         base = load_golden(str(fx["base"]))
         fx.update({k: v for k, v in base.items() if k.startswith("in.")})
+        if "config.n_scalars" in fx:
+            fx["in.scalars"] = fx["in.scalars"][: int(fx["config.n_scalars"])].copy()
     return fx
 
 
@@ -34,7 +36,8 @@ def golden_config(fx: dict) -> dict:
             "apvm_upwinding": float(fx.get("config.apvm_upwinding", 0.5))}
 
 
-VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1)]
+VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1),
+            ("l2_L12_notracers", 2)]
 
 
 def inputs(fx: dict) -> dict:

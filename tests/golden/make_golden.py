@@ -41,12 +41,14 @@ CASES = {
 }
 
 # Configuration variants on the inputs of a base case (outputs only; the
-# fixture names its base): name -> (base, sub steps, monotonic, apvm, steps)
+# fixture names its base): name -> (base, sub steps, monotonic, apvm, steps,
+# scalars kept)
 VARIANTS = {
-    "l2_L12_sub1": ("l2_L12", 1, True, 0.5, 2),     # one acoustic substep per stage
-    "l2_L12_sub4": ("l2_L12", 4, True, 0.5, 2),     # (1, 2, 4) substeps
-    "l2_L12_nomono": ("l2_L12", 2, False, 0.5, 2),  # standard RK3 transport
-    "l2_L12_noapvm": ("l2_L12", 2, True, 0.0, 1),   # no APVM upwinding
+    "l2_L12_sub1": ("l2_L12", 1, True, 0.5, 2, None),     # one acoustic substep per stage
+    "l2_L12_sub4": ("l2_L12", 4, True, 0.5, 2, None),     # (1, 2, 4) substeps
+    "l2_L12_nomono": ("l2_L12", 2, False, 0.5, 2, None),  # standard RK3 transport
+    "l2_L12_noapvm": ("l2_L12", 2, True, 0.0, 1, None),   # no APVM upwinding
+    "l2_L12_notracers": ("l2_L12", 2, True, 0.5, 2, 0),   # no scalars at all
 }
 
 
@@ -126,7 +128,7 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
             path = HERE / f"step_{name}.npz"
             np.savez_compressed(path, **out)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
-        for vname, (base, vsub, mono, apvm, vsteps) in VARIANTS.items():
+        for vname, (base, vsub, mono, apvm, vsteps, keep) in VARIANTS.items():
             if base != name or (only and vname not in only):
                 continue
             t0 = time.time()
@@ -136,7 +138,13 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
                                        config_apvm_upwinding=apvm)
             vout = {"base": np.array(base), "config.dt": dt, "config.n_sub_steps": vsub,
                     "config.monotonic": int(mono), "config.apvm_upwinding": apvm}
-            run(DryDycoreDriver, mesh, vg, ref, vcfg, ac, tm, wp, case, vsteps, "dry", vout)
+            vcase = case
+            if keep is not None:
+                import dataclasses
+
+                vcase = dataclasses.replace(case, scalars=case.scalars[:keep].copy())
+                vout["config.n_scalars"] = keep
+            run(DryDycoreDriver, mesh, vg, ref, vcfg, ac, tm, wp, vcase, vsteps, "dry", vout)
             path = HERE / f"step_{vname}.npz"
             np.savez_compressed(path, **vout)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")

@@ -67,6 +67,24 @@ def test_strict_step_matches_reference_variants(name, steps):
     drv.close()
 
 
+def test_tall_columns_match_oracle():
+    """130 levels (stride 136, 34 four-level chunks per column, more than a
+    warp): the column sweeps run in their one-level form (k_vcoef,
+    k_ac_cell) while every other kernel keeps four levels per thread."""
+    arr = case_arrays(build_case(build_mesh(2, lloyd=2, seed=0), n_levels=130, seed=0, n_condensates=1))
+    drv = make_driver(arr, 900.0, 2, "native")
+    orc = OracleDycore(arr, OracleConfig(dt=900.0, n_sub_steps=2, moist="native"))
+    state, side = State(*(np.asarray(arr[k]).copy() for k in STATE)), None
+    for step in (1, 2):
+        res = drv.step()
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), getattr(state, k)) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), getattr(side, k)) == 0, (step, k)
+    drv.close()
+
+
 @pytest.fixture(scope="module")
 def c1_case():
     mesh = build_mesh(4, lloyd=20, seed=0)

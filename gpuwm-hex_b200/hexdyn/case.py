@@ -431,6 +431,46 @@ def qsat(temperature: np.ndarray, pressure: np.ndarray) -> np.ndarray:
     return 0.622 * es / (pressure - 0.378 * es)
 
 
+def _libm_sinf():
+    import ctypes
+    import ctypes.util
+
+    name = ctypes.util.find_library("m")
+    if name is None:
+        return None
+    fn = ctypes.CDLL(name).sinf
+    fn.argtypes = [ctypes.c_float]
+    fn.restype = ctypes.c_float
+    return fn
+
+
+def vertical_velocity_damping(zgrid: np.ndarray, xnutr: float, zd: float) -> np.ndarray:
+    """Implicit w-damping coefficients dss [L][C] of MPAS-A v8.4.1
+    (``hexcore/damping_v841.py:23`` build_v841_vertical_velocity_damping,
+    float32 lane): above the layer midpoint height zd, dss = xnutr *
+    sin^2(pi/2 (z_mid - zd) / (z_top - zd)) with every operation in float32
+    and the sine from the C library's sinf, as the reference evaluates it."""
+    h = np.asarray(zgrid, dtype=F32)
+    nlev, ncell = h.shape[0] - 1, h.shape[1]
+    dss = np.zeros((nlev, ncell), dtype=F32)
+    x = F32(xnutr)
+    if x == F32(0.0):
+        return dss
+    half = F32(0.5)
+    pi = np.arccos(F32(-1.0))
+    start = F32(zd)
+    midpoint = half * (h[:-1] + h[1:])
+    active = midpoint > start
+    denominator = np.broadcast_to(h[-1] - start, midpoint.shape)
+    phase = (half * pi) * (midpoint[active] - start) / denominator[active]
+    sinf = _libm_sinf()
+    if sinf is None:
+        raise RuntimeError("the damping profile needs the C library's sinf")
+    sine = np.array([sinf(float(p)) for p in phase], dtype=F32)
+    dss[active] = x * (sine * sine)
+    return dss
+
+
 def build_case(mesh: VoronoiMesh, *, n_levels: int = 55, ztop: float = 30000.0,
                seed: int = 0, n_condensates: int = 0, jet_speed: float = 35.0,
                perturbation: float = 1.0, coef_3rd_order: float = 0.25,

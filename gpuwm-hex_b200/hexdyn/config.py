@@ -55,6 +55,7 @@ class DycoreConfig:
     config_smdiv: float = 0.1
     config_len_disp: float = 0.0
     config_xnutr: float = 0.0
+    config_zd: float = 22_000.0
     config_horiz_mixing: str = "off"
     config_moist_physics: bool = False
     config_rayleigh_damp_u: bool = False
@@ -138,9 +139,13 @@ class DycoreConfig:
         if not (lo >= 0.0 and hi > lo):
             _refuse("config_epssm_transition_top_z", (lo, hi), "the transition must have positive width",
                     "0<=bottom<top")
-        if self.config_xnutr != 0.0:
-            _refuse("config_xnutr", self.config_xnutr, "implicit upper-level w damping is not on this path yet",
-                    "config_xnutr=0.0")
+        # hexcore/driver.py:436-447 (V841DryDycoreConfig validation)
+        if not math.isfinite(self.config_xnutr) or not 0.0 <= self.config_xnutr <= 1.0:
+            _refuse("config_xnutr", self.config_xnutr, "v8.4.1 requires a finite bounded damping coefficient",
+                    "0.0<=config_xnutr<=1.0")
+        if not math.isfinite(self.config_zd) or self.config_zd <= 0.0:
+            _refuse("config_zd", self.config_zd, "v8.4.1 requires a finite positive damping start height",
+                    "config_zd>0")
         if self.config_horiz_mixing not in ("off", "2d_fixed"):
             _refuse("config_horiz_mixing", self.config_horiz_mixing,
                     "Smagorinsky mixing is outside this path (mixing is off in its configurations)",

@@ -29,6 +29,7 @@ from typing import Any
 import numpy as np
 
 from . import _lib
+from .case import vertical_velocity_damping
 from .config import ConfigurationRefusal, DycoreConfig
 
 F32 = np.float32
@@ -410,7 +411,8 @@ def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terra
         "fzm": _f32(vertical.fzm), "fzp": _f32(vertical.fzp),
         "rdzw": _f32(vertical.rdzw), "rdzu": _f32(vertical.rdzu),
         "zz": _f32(vertical.zz), "zxu": _f32(vertical.zxu),
-        "dss": np.zeros((nlev, ncells), dtype=F32),
+        # implicit w damping from the configuration (hexcore/driver.py:2417)
+        "dss": vertical_velocity_damping(np.asarray(vertical.zgrid), cfg.config_xnutr, cfg.config_zd),
         "zb_cell": _f32(terrain.zb_cell), "zb3_cell": _f32(terrain.zb3_cell),
         "rho_base": _f32(reference.rho_base), "rho_theta_base": _f32(reference.rho_theta_base),
         "exner_base": _f32(reference.exner_base),

@@ -17,7 +17,8 @@ def test_defaults_validate():
     (dict(config_split_dynamics_transport=False), "config_split_dynamics_transport"),
     (dict(config_smdiv=0.0), "config_smdiv"),
     (dict(config_divergence_damping=False), "config_divergence_damping"),
-    (dict(config_xnutr=0.2), "config_xnutr"),
+    (dict(config_xnutr=1.5), "config_xnutr"),
+    (dict(config_xnutr=0.2, config_zd=0.0), "config_zd"),
     (dict(config_horiz_mixing="2d_smagorinsky"), "config_horiz_mixing"),
     (dict(config_moist_physics=True), "config_moist_physics"),
     (dict(moist_coefficients="wet"), "moist_coefficients"),

@@ -32,10 +32,16 @@ def test_oracle_matches_reference_bitwise(name, label, steps):
 @pytest.mark.parametrize("name,steps", VARIANTS)
 def test_oracle_matches_reference_variants(name, steps):
     """Configuration variants (one and four acoustic substeps, standard RK3
-    transport, no APVM) against the reference run with that configuration."""
+    transport, no APVM, no tracers, implicit w damping) against the reference
+    run with that configuration."""
     fx = load_golden(name)
     c = golden_config(fx)
     arr = inputs(fx)
+    if c["xnutr"]:
+        from hexdyn.case import vertical_velocity_damping
+
+        arr["vertical.dss"] = vertical_velocity_damping(arr["vertical.zgrid"], c["xnutr"], c["zd"])
+        assert np.count_nonzero(arr["vertical.dss"]) > 0
     orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["n_sub_steps"], monotonic=c["monotonic"],
                                          apvm_upwinding=c["apvm_upwinding"], moist="dry"))
     state = State(*(arr[k].copy() for k in STATE))

@@ -32,6 +32,20 @@
   const int ent = (blockIdx.x / (nT)) * blockDim.y + threadIdx.y; \
   if (ent >= (n)) return;
 
+// Neighbour gathers: each iteration loads an index and then the neighbour's
+// levels, so unrolling lets the loads of several neighbours be in flight
+// together.  HEX_GATHER_UNROLL sets the unroll factor (0: the compiler's choice).
+#ifndef HEX_GATHER_UNROLL
+#define HEX_GATHER_UNROLL 2
+#endif
+#define HEX_PRAGMA(x) _Pragma(#x)
+#define HEX_UNROLL_N(n) HEX_PRAGMA(unroll n)
+#if HEX_GATHER_UNROLL > 0
+#define HEX_GATHER HEX_UNROLL_N(HEX_GATHER_UNROLL)
+#else
+#define HEX_GATHER
+#endif
+
 struct V4 {
   float a[4];
 };
@@ -122,6 +136,7 @@ __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ 
   const int n = g.deg[c];
   const float ia = g.inv_area[c];
   V4 ke = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float dd = g.dc[e] * g.dv[e];
@@ -131,6 +146,7 @@ __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ 
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] * ia * 0.625f;
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int vtx = g.voc[c * g.maxE + s];
     const float kt = (1.0f - 0.625f) * g.kite[3 * vtx + g.kite_slot[c * g.maxE + s]];
@@ -141,6 +157,7 @@ __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ 
   st4m(ke_out + c * S + k0, ke, k0, 0, g.L);
   if (g.apvm_on) {
     V4 pvc = v4zero();
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const int vtx = g.voc[c * g.maxE + s];
       const float kite = g.kite[3 * vtx + g.kite_slot[c * g.maxE + s]];
@@ -162,6 +179,7 @@ __global__ void HEX_VEC_BOUNDS kv_diag_edge(HexGeo g, const float* __restrict__ 
   if (recompute_v) {
     vt = v4zero();
     const int n = g.neoe[e];
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const float w = g.weights[e * g.maxE2 + s];
       const V4 un = ld4(u + g.eoe[e * g.maxE2 + s] * S + k0);
@@ -228,6 +246,7 @@ __global__ void HEX_VEC_BOUNDS kv_euler_edge(HexGeo g, const float* __restrict__
 __device__ __forceinline__ V4 mass_flux_div4(const HexGeo& g, const float* __restrict__ ru, int c, int k0) {
   V4 acc = v4zero();
   const int n = g.deg[c];
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float sd = g.csign[c * g.maxE + s] * g.dv[e];
@@ -302,6 +321,7 @@ __global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ r
     cw[j] = g.coef3 * copysignf(1.0f, rui);
   }
   V4 at = v4zero(), aw = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int cs = cells[s] * S + k0;
     const float A = a1[s], B = a3[s];
@@ -343,6 +363,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_u(HexGeo g, const float* __restrict__ u, 
   const int n = g.neoe[e];
   const V4 pve = ld4(pv_edge + e * S + k0);
   V4 q = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int nb = g.eoe[e * g.maxE2 + s];
     const float w = g.weights[e * g.maxE2 + s];
@@ -361,6 +382,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_u(HexGeo g, const float* __restrict__ u, 
   for (int j = 0; j < 4; ++j) need = need || !(fabsf(q.a[j]) > 0.0f);
   if (need) {
     const float fe = g.f_edge[e];
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const int nb = g.eoe[e * g.maxE2 + s];
       const float w = g.weights[e * g.maxE2 + s];
@@ -431,6 +453,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
   const float* cs = g.csign + c * g.maxE;
   // horizontal parts: rho-theta flux divergence, RK>1 correction, w flux
   V4 res = v4zero(), hres = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = eoc[s];
     const float sg = cs[s];
@@ -447,6 +470,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
   }
   if (rk_step > 1) {
     const V4 tc = ld4(theta_s + c * S + k0);
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const int e = eoc[s];
       const int e0 = g.coe[2 * e], e1 = g.coe[2 * e + 1];
@@ -485,6 +509,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
     }
   }
   // omega conversion (interfaces 1..L-1)
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = eoc[s];
     const float sg = cs[s];
@@ -691,6 +716,7 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
   // the next stage's mass-flux divergence of ru_new (mass_flux_div4, the
   // same operands in the same order) accumulates in the same edge loop
   V4 hd = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float sign = g.csign[c * g.maxE + s];
@@ -751,14 +777,24 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
 }
 
 // ------------------------------------------------------------ transport
-// hexcore/transport.py:1461 third-order edge values, one tracer per block
-// row.  mono: the monotonic source flux (velocity folded in; the literal
-// ten-term association for ten-cell stencils).
+// hexcore/transport.py:1461 third-order edge values.  A thread serves
+// HEX_TR_GROUP tracers at its four levels: the stencil indices, the two
+// coefficient tables and the per-level weights (coefficient + sign(u) x
+// third-order coefficient) are loaded and formed once per stencil cell and
+// applied to every tracer of the group; block b serves tracer group
+// b % groups.  mono: the monotonic source flux (velocity folded in; the
+// literal ten-term association for ten-cell stencils).
+#ifndef HEX_TR_GROUP
+#define HEX_TR_GROUP 3
+#endif
 __global__ void HEX_VEC_BOUNDS kv_tr_edge(HexGeo g, int nT, int mono, const float* __restrict__ q, const float* __restrict__ hv,
                            float* __restrict__ out) {
-  HEX_VEC_TRACER(g.nE, nT)
+  HEX_VEC_TRACER(g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP)
+  constexpr int TG = HEX_TR_GROUP;
   const int e = ent, S = g.S;
-  const float* qt = q + (size_t)tr * g.nC * S;
+  const int t0 = tr * TG;
+  const size_t tstride = (size_t)g.nC * S;
+  const float* qg = q + (size_t)t0 * tstride + k0;
   const int n = g.n_adv[e];
   const int* cells = g.adv_cells + (size_t)e * g.advW;
   const float* a1 = g.adv + (size_t)e * g.advW;
@@ -767,36 +803,66 @@ __global__ void HEX_VEC_BOUNDS kv_tr_edge(HexGeo g, int nT, int mono, const floa
   float cs[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) cs[j] = g.coef3 * copysignf(1.0f, vel.a[j]);
-  V4 res;
+  V4 res[TG];
   if (mono && n == 10) {
-    V4 val;
     {
-      const V4 qv = ld4(qt + cells[0] * S + k0);
+      const float* qc = qg + cells[0] * S;
+      const float A = a1[0], B = a3[0];
+      float w[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) val.a[j] = (a1[0] + cs[j] * a3[0]) * qv.a[j];
+      for (int j = 0; j < 4; ++j) w[j] = A + cs[j] * B;
+#pragma unroll
+      for (int t = 0; t < TG; ++t)
+        if (t0 + t < nT) {
+          const V4 qv = ld4(qc + t * tstride);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) res[t].a[j] = w[j] * qv.a[j];
+        }
     }
+    HEX_GATHER
     for (int s = 1; s < 10; ++s) {
-      const V4 qv = ld4(qt + cells[s] * S + k0);
+      const float* qc = qg + cells[s] * S;
       const float A = a1[s], B = a3[s];
+      float w[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) val.a[j] = val.a[j] + (A + cs[j] * B) * qv.a[j];
+      for (int j = 0; j < 4; ++j) w[j] = A + cs[j] * B;
+#pragma unroll
+      for (int t = 0; t < TG; ++t)
+        if (t0 + t < nT) {
+          const V4 qv = ld4(qc + t * tstride);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) res[t].a[j] = res[t].a[j] + w[j] * qv.a[j];
+        }
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) res.a[j] = vel.a[j] * val.a[j];
+    for (int t = 0; t < TG; ++t)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) res[t].a[j] = vel.a[j] * res[t].a[j];
   } else {
-    res = v4zero();
+#pragma unroll
+    for (int t = 0; t < TG; ++t) res[t] = v4zero();
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
-      const V4 qv = ld4(qt + cells[s] * S + k0);
+      const float* qc = qg + cells[s] * S;
       const float A = a1[s], B = a3[s];
+      float w[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        float wgt = A + cs[j] * B;
-        if (mono) wgt = vel.a[j] * wgt;
-        res.a[j] = res.a[j] + wgt * qv.a[j];
+        w[j] = A + cs[j] * B;
+        if (mono) w[j] = vel.a[j] * w[j];
       }
+#pragma unroll
+      for (int t = 0; t < TG; ++t)
+        if (t0 + t < nT) {
+          const V4 qv = ld4(qc + t * tstride);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) res[t].a[j] = res[t].a[j] + w[j] * qv.a[j];
+        }
     }
   }
-  st4m(out + (size_t)tr * g.nE * S + e * S + k0, res, k0, 0, g.L);
+#pragma unroll
+  for (int t = 0; t < TG; ++t)
+    if (t0 + t < nT) st4m(out + (size_t)(t0 + t) * g.nE * S + e * S + k0, res[t], k0, 0, g.L);
 }
 
 // transport vertical flux at interface j = k0 + d (hexcore/transport.py:1389).
@@ -823,6 +889,7 @@ __global__ void HEX_VEC_BOUNDS kv_tr_std(HexGeo g, int nT, float step, float wn,
   const float* ev = edge_q + (size_t)tr * g.nE * S;
   const int n = g.deg[c];
   V4 t = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float ts = -g.csign[c * g.maxE + s];
@@ -858,6 +925,7 @@ __global__ void HEX_VEC_BOUNDS kv_fct_target(HexGeo g, float step, const float* 
   const int n = g.deg[c];
   const float ia = g.inv_area[c];
   V4 hd = v4zero();
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float ts = -g.csign[c * g.maxE + s];
@@ -917,6 +985,7 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
     mx[j] = fmaxf(fmaxf(a, o), b);
   }
   const int n = g.deg[c];
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const V4 on = ld4(ot + g.coc[c * g.maxE + s] * S + k0);
 #pragma unroll
@@ -940,6 +1009,7 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
     s_out[j] = -g.rdzw[k] * (pos0(vr[j + 1]) - neg0(vr[j]));
   }
   const float ia = g.inv_area[c];
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float ts = -g.csign[c * g.maxE + s];
@@ -1008,6 +1078,7 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell2(HexGeo g, int nT, float step, const 
   V4 mass = ld4(mass_in + toff + ii);
   const int n = g.deg[c];
   const float ia = g.inv_area[c];
+  HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
     const float ts = -g.csign[c * g.maxE + s];
@@ -1236,6 +1307,7 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
     const int n = g.deg[c];
     const float ia = g.inv_area[c];
     const V4 tc = ld4(theta_s + ii);
+    HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const int e = g.eoc[c * g.maxE + s];
       const int e0 = g.coe[2 * e], e1 = g.coe[2 * e + 1];

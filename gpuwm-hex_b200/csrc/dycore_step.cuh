@@ -226,13 +226,15 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
       if (si < 2 || !ctx.monotonic) {
         const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
-        LPST(L, g.nE, nT, tr_edge, g, 0, q_prev, (const float*)w.flux_u, w.edge_q);
+        L.lpvt("k_tr_edge", g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP, kv_tr_edge, g, nT, 0, q_prev,
+               (const float*)w.flux_u, w.edge_q);
         LPST(L, g.nC, nT, tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)out.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, q_next);
       } else {
         LPS(L, g.nC, 1, fct_target, g, step, (const float*)in.rho, (const float*)w.flux_u,
              (const float*)w.flux_w, w.target, w.flag);
-        LPST(L, g.nE, nT, tr_edge, g, 1, q_prev, (const float*)w.flux_u, w.edge_q);
+        L.lpvt("k_tr_edge", g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP, kv_tr_edge, g, nT, 1, q_prev,
+               (const float*)w.flux_u, w.edge_q);
         LPST(L, g.nC, nT, fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
              (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass);

@@ -331,10 +331,11 @@ def run_ensemble(args, stream, dist, world: int, rank: int, plain_case) -> dict:
 
 # ------------------------------------------------------ learned corrector
 def run_learned(args, plain_case) -> dict:
-    """The learned-corrector path on this mesh (qv + 2 condensates, dt 720 s):
-    pairs from 4 members, 30 epochs per network, then half a simulated day
-    of the plain, reduced-with-checks and learned paths from a held-out
-    member.  The 5-day evaluation is ``python -m hexdyn.learned_eval``."""
+    """The learned-corrector path on this mesh (qv + 2 condensates, plain dt
+    720 s; reduced step dt 1440 s with 3 substeps standing for two plain
+    steps): pairs from 4 members, 30 epochs per network, then half a
+    simulated day of the plain, reduced-with-checks and learned paths from a
+    held-out member.  The 5-day evaluation is ``python -m hexdyn.learned_eval``."""
     from hexdyn.learned_eval import run
 
     res = run(level=args.level, levels=args.levels, members=4, epochs=30, days=0.5, mesh=plain_case.mesh)

@@ -1,13 +1,17 @@
-"""Learned corrector: a reduced-substep step plus per-column and per-edge
+"""Learned corrector: a cheap reduced step plus per-column and per-edge
 BF16 tensor-core networks, with the full step as fallback.
 
-The reduced step runs the same dycore with fewer acoustic substeps
-(``config_number_of_sub_steps`` 1 instead of 2).  After it, a column
+The reduced step runs the same dycore either with a time step ``ratio``
+times longer and ``ratio`` times as many acoustic substeps (the acoustic
+step and its stability unchanged, the large-step tendencies, recovery and
+transport done once instead of ``ratio`` times), or with fewer acoustic
+substeps at the same time step (``ratio`` 1).  It stands for ``ratio``
+full steps.  After it, a column
 network (inputs theta_m, rho_zz, w, qv, the cell mean of edge u and the
 neighbour mean of theta_m over the levels; 3 hidden layers; outputs the
 increments of theta_m, rho_zz and w) and an edge network (inputs u, theta_m
 of both cells and their mean rho_zz; outputs the increment of u) correct
-the state towards what the full step would have produced.  The networks
+the state towards what the ``ratio`` full steps would have produced.  The networks
 are trained on pairs of full and reduced steps taken from the same state
 (:func:`make_pairs`), entirely with the library's kernels (hexdyn.mlp).
 
@@ -51,6 +55,16 @@ def snapshot(drv: HexDycoreDriver) -> dict:
     return {n: atm.padded(n).clone() for n in FIELDS if not (n == "scalars" and drv.sizes["n_scalars"] == 0)}
 
 
+def snapshot_into(drv: HexDycoreDriver, snap: dict | None) -> dict:
+    """Snapshot into the buffers of an earlier snapshot of the same driver."""
+    if snap is None:
+        return snapshot(drv)
+    atm = DeviceAtmosphere(drv)
+    for n, t in snap.items():
+        t.copy_(atm.padded(n))
+    return snap
+
+
 def restore(drv: HexDycoreDriver, snap: dict) -> None:
     atm = DeviceAtmosphere(drv)
     for n, t in snap.items():
@@ -88,12 +102,13 @@ class Pairs:
 
 
 def make_pairs(full: HexDycoreDriver, reduced: HexDycoreDriver, states, *, samples: int, steps_between: int = 2,
-               times: int = 2, seed: int = 0) -> Pairs:
+               times: int = 2, seed: int = 0, ratio: int = 1) -> Pairs:
     """From each initial state (``(state, saved_diagnostics or None)``),
-    advance the full driver and, ``times`` times, take one full and one
-    reduced step from the same state; sample ``samples`` columns and edges
-    in total.  Features are those of the reduced result, targets the
-    difference full - reduced of theta_m, rho_zz, w (columns) and u (edges)."""
+    advance the full driver and, ``times`` times, take ``ratio`` full steps
+    and one reduced step from the same state; sample ``samples`` columns
+    and edges in total.  Features are those of the reduced result, targets
+    the difference full - reduced of theta_m, rho_zz, w (columns) and u
+    (edges)."""
     import torch
 
     t0 = time.perf_counter()
@@ -109,7 +124,7 @@ def make_pairs(full: HexDycoreDriver, reduced: HexDycoreDriver, states, *, sampl
             full.step_async(steps_between)
             copy_state(reduced, full)
             reduced.step_async(1)
-            full.step_async(1)
+            full.step_async(ratio)
             f_full.compute(full)
             f_red.compute(reduced)
             full.synchronize()
@@ -229,14 +244,17 @@ class TrainedNet:
 
 
 class LearnedStepper:
-    """Runs the corrected reduced step on ``reduced``; ``full`` is the
-    fallback.  ``z_mid`` is the height of every cell level, padded layout."""
+    """Runs the corrected reduced step on ``reduced``; ``ratio`` full steps
+    are the fallback.  ``z_mid`` is the height of every cell level, padded
+    layout."""
 
     def __init__(self, full: HexDycoreDriver, reduced: HexDycoreDriver, col: TrainedNet, edge: TrainedNet, z_mid,
-                 *, energy_tol: float = 1e-4, w_growth_tol: float = 0.05, use_network: bool = True):
+                 *, energy_tol: float = 1e-4, w_growth_tol: float = 0.05, use_network: bool = True,
+                 ratio: int = 1):
         import torch
 
         self.full, self.reduced, self.col, self.edge = full, reduced, col, edge
+        self.ratio = int(ratio)
         self.z = z_mid
         self.tol = energy_tol
         self.w_tol = w_growth_tol
@@ -253,6 +271,14 @@ class LearnedStepper:
         self.steps = 0
         self.last_rel = []
         self.last_growth = []
+        self._snap = None
+        self._energy_known = False  # slot 0 already holds the energy of the current state
+
+    def reset(self) -> None:
+        """Forget counters and the cached energy (after the state was set)."""
+        self.fallbacks, self.flagged, self.steps, self.first_fallback = 0, 0, 0, None
+        self.last_rel, self.last_growth = [], []
+        self._energy_known = False
 
     def total_energy(self, drv: HexDycoreDriver, slot: int) -> None:
         lib = _lib.load()
@@ -277,11 +303,14 @@ class LearnedStepper:
 
     def step(self) -> bool:
         """One corrected step; returns False when it fell back to the full
-        step (the reduced step's validation flag was set, or the energy
-        changed by more than the tolerance)."""
+        steps (the reduced step's validation flag was set, the energy
+        changed by more than the tolerance or the RMS of w grew too fast)."""
         lib = _lib.load()
-        snap = snapshot(self.reduced)
-        self.total_energy(self.reduced, 0)
+        snap = self._snap = snapshot_into(self.reduced, self._snap)
+        if self._energy_known:
+            self.energy[0:2].copy_(self.energy[2:4])  # the last step's result is this step's start
+        else:
+            self.total_energy(self.reduced, 0)
         self.reduced.step_async(1)
         if self.use_network:
             self.correct()
@@ -302,10 +331,11 @@ class LearnedStepper:
             self.flagged += 1
         if not ok and self.first_fallback is None:
             self.first_fallback = self.steps - 1
+        self._energy_known = ok
         if not ok:
             self.fallbacks += 1
             restore(self.full, snap)
-            self.full.step_async(1)
+            self.full.step_async(self.ratio)
             copy_state(self.reduced, self.full)
             rc = lib.hexdyn_read_flag(self.full._handle, self.full._stream_handle(), C.byref(flag))
             if rc == _lib.HEXDYN_E_NUMERIC:

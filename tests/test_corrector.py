@@ -1,11 +1,13 @@
 """The learned-corrector pipeline on a small mesh: pairs of full and reduced
 steps, training of both networks with the tensor-core kernels, and corrected
-steps with their checks and fallback.
+steps with their checks and fallback, for both reduced steps (one substep
+at the same time step; a doubled time step with three substeps standing for
+two full steps).
 
 What the networks gain is measured on held-out pairs: their error on the
-increments (full step minus reduced step) must be below the error of
-applying no correction.  (Whether that pays off over days is reported by
-``python -m hexdyn.learned_eval``; on the 40962-cell mesh it does not.)
+increments (full steps minus reduced step) must be below the error of
+applying no correction.  The forecast errors over days are reported by
+``python -m hexdyn.learned_eval``.
 """
 
 import numpy as np
@@ -14,7 +16,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_corrector_trains_and_steps():
+@pytest.mark.parametrize("ratio,red_substeps", [(1, 1), (2, 3)])
+def test_corrector_trains_and_steps(ratio, red_substeps):
     import torch
 
     import hexdyn
@@ -30,8 +33,9 @@ def test_corrector_trains_and_steps():
     base = build_case(mesh, n_levels=L, seed=0, n_condensates=2)
     members = [build_case(mesh, n_levels=L, seed=10 + i, n_condensates=2, theta_noise=0.1, like=base) for i in range(3)]
     full = hexdyn.from_case(base, DycoreConfig(config_dt=1200.0, config_number_of_sub_steps=2), capture_graph=True)
-    red = hexdyn.from_case(base, DycoreConfig(config_dt=1200.0, config_number_of_sub_steps=1), capture_graph=True)
-    pairs = make_pairs(full, red, [(m, None) for m in members], samples=1536, times=2)
+    red = hexdyn.from_case(base, DycoreConfig(config_dt=1200.0 * ratio, config_number_of_sub_steps=red_substeps),
+                           capture_graph=True)
+    pairs = make_pairs(full, red, [(m, None) for m in members], samples=1536, times=2, ratio=ratio)
     assert pairs.col_x.shape == (1536, 6 * L) and pairs.col_y.shape == (1536, 3 * L)
     assert np.all(np.isfinite(pairs.col_x)) and np.all(np.isfinite(pairs.edge_y))
     col = TrainedNet(6 * L, 128, 3, 3 * L, seed=1)
@@ -43,7 +47,7 @@ def test_corrector_trains_and_steps():
     assert re.val_loss < re.val_loss_zero, (re.val_loss, re.val_loss_zero)
     # corrected steps with the checks; every step ends finite
     red.set_state(members[0])
-    stepper = LearnedStepper(full, red, col, edge, _z_mid_padded(base, red.level_stride))
+    stepper = LearnedStepper(full, red, col, edge, _z_mid_padded(base, red.level_stride), ratio=ratio)
     for _ in range(4):
         stepper.step()
     st, _ = red.get_state()

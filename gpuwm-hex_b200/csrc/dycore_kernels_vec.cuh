@@ -17,6 +17,22 @@
 #define HEX_VEC_MIN_BLOCKS 4
 #endif
 #define HEX_VEC_BOUNDS __launch_bounds__(256, HEX_VEC_MIN_BLOCKS)
+// Kernels measured faster at another cap: the momentum tendency (a
+// latency-bound ten-point gather) at 6 blocks (40 registers), the tracer
+// edge values (three tracers' accumulators per thread) at 2 (128), the
+// limited antidiffusive flux at 6 and the standard tracer update at 5.
+#ifndef HEX_TEND_U_MIN_BLOCKS
+#define HEX_TEND_U_MIN_BLOCKS 6
+#endif
+#ifndef HEX_TR_EDGE_MIN_BLOCKS
+#define HEX_TR_EDGE_MIN_BLOCKS 2
+#endif
+#ifndef HEX_FCT_EDGE_MIN_BLOCKS
+#define HEX_FCT_EDGE_MIN_BLOCKS 6
+#endif
+#ifndef HEX_TR_STD_MIN_BLOCKS
+#define HEX_TR_STD_MIN_BLOCKS 5
+#endif
 
 #define HEX_VEC_PARALLEL(n)                                \
   const int k0 = threadIdx.x * 4;                          \
@@ -348,7 +364,7 @@ __device__ __forceinline__ float wduz_win(const HexGeo& g, const Win& uw, const 
 }
 
 // tend_ru: vertical transport + hexcore/dynamics_v841.py:121 momentum + saved Euler.
-__global__ void HEX_VEC_BOUNDS kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
+__global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
                           const float* __restrict__ rho, const float* __restrict__ pv_edge,
                           const float* __restrict__ ke, const float* __restrict__ hdiv,
                           const float* __restrict__ euler_ru, float* __restrict__ tend_ru) {
@@ -787,7 +803,7 @@ __global__ void HEX_VEC_BOUNDS kv_recover_cell(HexGeo g, int stage3, const float
 #ifndef HEX_TR_GROUP
 #define HEX_TR_GROUP 3
 #endif
-__global__ void HEX_VEC_BOUNDS kv_tr_edge(HexGeo g, int nT, int mono, const float* __restrict__ q, const float* __restrict__ hv,
+__global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo g, int nT, int mono, const float* __restrict__ q, const float* __restrict__ hv,
                            float* __restrict__ out) {
   HEX_VEC_TRACER(g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP)
   constexpr int TG = HEX_TR_GROUP;
@@ -877,7 +893,7 @@ __device__ __forceinline__ float tr_vflux_win(const HexGeo& g, const Win& q, con
 }
 
 // hexcore/transport.py:1649 advance_scalars (RK1/RK2 of split transport).
-__global__ void HEX_VEC_BOUNDS kv_tr_std(HexGeo g, int nT, float step, float wn, const float* __restrict__ q_old,
+__global__ void __launch_bounds__(256, HEX_TR_STD_MIN_BLOCKS) kv_tr_std(HexGeo g, int nT, float step, float wn, const float* __restrict__ q_old,
                           const float* __restrict__ q_stage, const float* __restrict__ rho_old,
                           const float* __restrict__ rho_new, const float* __restrict__ hv,
                           const float* __restrict__ ww, const float* __restrict__ edge_q,
@@ -1041,7 +1057,7 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
 }
 
 // hexcore/transport.py:1919-2118: the limited antidiffusive edge flux.
-__global__ void HEX_VEC_BOUNDS kv_fct_edge(HexGeo g, int nT, float step, const float* __restrict__ q_old, const float* __restrict__ hv,
+__global__ void __launch_bounds__(256, HEX_FCT_EDGE_MIN_BLOCKS) kv_fct_edge(HexGeo g, int nT, float step, const float* __restrict__ q_old, const float* __restrict__ hv,
                             const float* __restrict__ high_e, const float* __restrict__ scale_in,
                             const float* __restrict__ scale_out, float* __restrict__ hres_lim) {
   HEX_VEC_TRACER(g.nE, nT)

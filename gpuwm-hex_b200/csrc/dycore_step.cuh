@@ -8,6 +8,45 @@ struct Launcher {
   std::vector<HexProfEvent>* prof = nullptr;  // per-launch CUDA events when profiling
   long long count = 0;
   cudaError_t err = cudaSuccess;
+  cudaStream_t main_st = nullptr;  // the caller's stream while launches go to the side stream
+  bool on_side = false;            // (the caller's stream may be the legacy stream, handle 0)
+  int next_event = 0;
+  // Independent kernels: fork() makes the side stream wait for everything
+  // launched so far, side() sends the following launches there, and
+  // join() makes the caller's stream wait for them.  Serial (no-ops) when
+  // the context has no side stream or launches are being profiled.
+  int region = 0;  // the forked region being launched (bit of ctx.concurrent_regions)
+  bool concurrent() const {
+    return ctx.side_stream != nullptr && prof == nullptr && (ctx.concurrent_regions & region);
+  }
+  void signal(cudaStream_t from, cudaStream_t to) {
+    if (err != cudaSuccess) return;
+    cudaEvent_t ev = ctx.fork_events[next_event++ & 3];
+    err = cudaEventRecord(ev, from);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(to, ev, 0);
+  }
+  void fork() {
+    if (concurrent()) signal(st, ctx.side_stream);
+  }
+  void side() {
+    if (concurrent() && !on_side) {
+      main_st = st;
+      st = ctx.side_stream;
+      on_side = true;
+    }
+  }
+  void main() {
+    if (on_side) {
+      st = main_st;
+      main_st = nullptr;
+      on_side = false;
+    }
+  }
+  void join() {
+    if (!concurrent()) return;
+    main();
+    signal(ctx.side_stream, st);
+  }
   // entities per block for tpe threads per entity under the label's block size
   int epb(const char* name, int tpe) const {
     const int threads = ctx.threads_for(name);
@@ -135,34 +174,46 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
     // bit 1 last subcycle (multiply by 1/splits after the sum)
     const int flux_mode = 4 | (sub == 0 ? 1 : 0) | (last ? 2 : 0);
     // vertical coefficients before RK (stage-1 acoustic dts, saved theta)
+    // (the saved Euler terms on the side stream: they share no array with
+    // the coefficients)
+    L.region = 1;
+    L.fork();
     {
       LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, ctx.dyn[0].dts2, (const float*)s_in->exner, (const float*)s_in->theta_m,
            (const float*)s_in->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
            w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
     }
+    L.side();
     LPS(L, g.nE, 1, euler_edge, g, (const float*)s_in->pressure_p, (const float*)s_in->rho_p,
          (const float*)w.qtot, (const float*)w.cqu, w.euler_ru);
     LPS(L, g.nC, 1, euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
          (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
          w.tend_rho, w.euler_rw);
+    L.join();
 
     const HexState* cur = saved;
     const HexSide* cs = s_in;
     for (int si = 0; si < 3; ++si) {
       const HexStage& stg = ctx.dyn[si];
       const float dts = (float)stg.acoustic_dt;
+      // the mass-flux divergence of cur->rho_u: computed by the previous
+      // stage's recovery, except for the first stage of the step
+      if (sub == 0 && si == 0) LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
+      // edge values, the momentum tendency and (stage 2) the coefficients
+      // are independent: the first on this stream, the others on the side
+      L.region = 2;
+      L.fork();
+      LPS(L, g.nE, 1, edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
+           w.edge_theta, w.edge_w);
+      L.side();
+      LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
+           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
       if (stg.stage == 2) {
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
       }
-      // the mass-flux divergence of cur->rho_u: computed by the previous
-      // stage's recovery, except for the first stage of the step
-      if (sub == 0 && si == 0) LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
-      LPS(L, g.nE, 1, edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
-           w.edge_theta, w.edge_w);
-      LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
-           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
+      L.join();
       LPS(L, g.nC, 1, tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
            (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
@@ -205,11 +256,16 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       LPS(L, g.nE, 1, recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
            (const float*)w.ru_avg, (const float*)s_in->rho_p, (const float*)w.rho_pp, o.rho_u, so.u, w.flux_u,
            fm, inv_steps, inv_splits);
+      // the cell recovery and the diagnostics of the new u share no array
+      L.region = 4;
+      L.fork();
       LPS(L, g.nC, 1, recover_cell, g, stg.stage == 3 ? 1 : 0, (const float*)s_in->rho_p,
            (const float*)s_in->rtheta_p, (const float*)saved->rho_w, (const float*)w.rho_pp, rtpp_final,
            (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
            inv_splits, w.flag, w.hdiv);
+      L.side();
       diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
+      L.join();
       cur = &o;
       cs = &so;
     }

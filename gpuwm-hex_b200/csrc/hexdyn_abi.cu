@@ -473,6 +473,13 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
   }
   HEX_CUDA(cudaMallocHost(&h->host_flag, sizeof(int)), "host flag");
   *h->host_flag = 0;
+  // HEXDYN_CONCURRENT=0 keeps every launch of a step on the caller's stream
+  const char* conc = getenv("HEXDYN_CONCURRENT");
+  if (conc) c.concurrent_regions = atoi(conc);
+  if (c.concurrent_regions != 0) {
+    HEX_CUDA(cudaStreamCreateWithFlags(&c.side_stream, cudaStreamNonBlocking), "side stream");
+    for (auto& ev : c.fork_events) HEX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "fork event");
+  }
   HEX_CUDA(cudaDeviceSynchronize(), "create");
   return HEXDYN_OK;
 }
@@ -825,6 +832,9 @@ int hexdyn_destroy(HexDynHandle* h) {
     if (c.graph[p]) cudaGraphDestroy(c.graph[p]);
   }
   for (void* p : c.allocations) cudaFree(p);
+  for (auto& ev : c.fork_events)
+    if (ev) cudaEventDestroy(ev);
+  if (c.side_stream) cudaStreamDestroy(c.side_stream);
   if (h->host_flag) cudaFreeHost(h->host_flag);
   if (h->batch_fork) cudaEventDestroy(h->batch_fork);
   if (h->batch_done) cudaEventDestroy(h->batch_done);

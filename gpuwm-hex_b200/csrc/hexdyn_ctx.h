@@ -84,6 +84,11 @@ struct HexCtx {
   // while the autotuner times a candidate.
   std::vector<std::pair<std::string, int>> tuned_threads;
   int force_threads = 0;
+  // Second stream for independent kernels of a stage (fork/join by events,
+  // captured into the step graph as parallel branches); null: one stream.
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_events[4] = {nullptr, nullptr, nullptr, nullptr};
+  int concurrent_regions = 7;  // bit mask of the forked regions of a step
   int threads_for(const char* label) const {
     if (force_threads) return force_threads;
     for (const auto& t : tuned_threads)

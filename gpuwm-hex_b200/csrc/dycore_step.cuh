@@ -208,7 +208,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       L.side();
       LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
            (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
-      if (stg.stage == 2) {
+      if (stg.stage == 2 && ctx.order == 3) {  // hexcore/driver.py:2894
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
              w.cofwt, w.a_tri, w.alpha_tri, w.gamma_tri, w.flag);
@@ -281,7 +281,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const float step = (float)stg.large_dt;
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
       if (si < 2 || !ctx.monotonic) {
-        const float wn = si == 0 ? (float)(1.0 / 3.0) : (si == 1 ? 0.5f : 1.0f);
+        // hexcore/transport.py:1749-1755 time-interpolation weight of rho_new
+        const float wn = si == 0 ? (ctx.order == 3 ? (float)(1.0 / 3.0) : 0.5f) : (si == 1 ? 0.5f : 1.0f);
         L.lpvt("k_tr_edge", g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP, kv_tr_edge, g, nT, 0, q_prev,
                (const float*)w.flux_u, w.edge_q);
         LPST(L, g.nC, nT, tr_std, g, step, wn, (const float*)in.scalars, q_prev, (const float*)in.rho,

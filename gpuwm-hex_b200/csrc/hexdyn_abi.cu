@@ -242,6 +242,8 @@ int validate(const HexDynDesc* d) {
                 "compiled maxima 8 / 16 / 16", d->max_edges, d->max_edges2, d->adv_width);
   if (!(d->dt > 0.0) || !isfinite(d->dt)) return fail(HEXDYN_E_ARG, "config_dt=%g must be finite and positive", d->dt);
   if (d->n_sub_steps < 1) return fail(HEXDYN_E_ARG, "config_number_of_sub_steps=%d must be positive", d->n_sub_steps);
+  if (d->time_integration_order != 0 && d->time_integration_order != 2 && d->time_integration_order != 3)
+    return fail(HEXDYN_E_ARG, "config_time_integration_order=%d: only 2 and 3 exist", d->time_integration_order);
   if (d->split_steps != 1 && d->split_steps != 3)
     return fail(HEXDYN_E_ARG, "config_dynamics_split_steps=%d: only 1 and 3 are implemented", d->split_steps);
   if (d->moist != 0 && d->moist != 1) return fail(HEXDYN_E_ARG, "moist=%d must be 0 or 1", d->moist);
@@ -424,13 +426,17 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
   for (int k = 0; k < L; ++k)
     if (d.u_init[k] != 0.0f || d.v_init[k] != 0.0f) g.winds_zero = 0;
 
-  // schedules (hexcore/integration.py:104 RKSchedule.from_mpas, order 3)
+  // schedules (hexcore/integration.py:104 RKSchedule.from_mpas): order 3
+  // (dt/3, dt/2, dt; one substep of dt/3, then n/2 and n of dt/n) or order
+  // 2 (dt/2, dt/2, dt; n/2, n/2 and n substeps of dt/n)
+  c.order = d.time_integration_order == 2 ? 2 : 3;
   const double dt_dyn = d.dt / d.split_steps;
   const int n = d.n_sub_steps;
-  const double large[3] = {dt_dyn / 3.0, dt_dyn / 2.0, dt_dyn};
-  const double acoustic[3] = {dt_dyn / 3.0, dt_dyn / n, dt_dyn / n};
-  const int counts[3] = {1, std::max(1, n / 2), n};
-  const double slarge[3] = {d.dt / 3.0, d.dt / 2.0, d.dt};
+  const bool rk2 = c.order == 2;
+  const double large[3] = {dt_dyn / (rk2 ? 2.0 : 3.0), dt_dyn / 2.0, dt_dyn};
+  const double acoustic[3] = {rk2 ? dt_dyn / n : dt_dyn / 3.0, dt_dyn / n, dt_dyn / n};
+  const int counts[3] = {rk2 ? std::max(1, n / 2) : 1, std::max(1, n / 2), n};
+  const double slarge[3] = {d.dt / (rk2 ? 2.0 : 3.0), d.dt / 2.0, d.dt};
   for (int i = 0; i < 3; ++i) {
     const float dts = (float)acoustic[i];
     const float dts2 = d.acoustic_dts2[i] != 0.0f ? d.acoustic_dts2[i] : dts * dts;
@@ -877,7 +883,9 @@ int check_compatible(const HexDynDesc& a, const HexDynDesc& b, int m) {
   if (b.n_levels != L) return bad("n_levels");
   if (b.n_scalars != a.n_scalars) return bad("n_scalars");
   if (b.dt != a.dt) return bad("dt");
-  if (b.n_sub_steps != a.n_sub_steps || b.split_steps != a.split_steps) return bad("the schedule");
+  if (b.n_sub_steps != a.n_sub_steps || b.split_steps != a.split_steps ||
+      (b.time_integration_order == 2) != (a.time_integration_order == 2))
+    return bad("the schedule");
   if (b.monotonic != a.monotonic || b.moist != a.moist || b.numerics != a.numerics) return bad("the options");
   const float fa[] = {a.coef_3rd_order, a.apvm_upwinding, a.smdiv, a.len_disp, a.epssm_minimum, a.epssm_maximum,
                       a.epssm_bottom_z, a.epssm_top_z, a.rgas, a.cp, a.gravity, a.p0, a.cf1, a.cf2, a.cf3,
@@ -1519,6 +1527,7 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   c.n_scalars = src.n_scalars;
   c.dt = src.dt;
   c.split_steps = src.split_steps;
+  c.order = src.order;
   c.monotonic = src.monotonic;
   c.geo = src.geo;
   for (int i = 0; i < 3; ++i) {

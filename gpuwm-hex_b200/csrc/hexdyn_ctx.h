@@ -64,6 +64,7 @@ struct HexCtx {
   int n_scalars;
   double dt;
   int split_steps;
+  int order = 3;        // config_time_integration_order (2 or 3)
   int monotonic;
   HexGeo geo;
   HexStage dyn[3];      // dynamics subcycle schedule

@@ -10,7 +10,7 @@ from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libhexdyn.so"
 
-HEXDYN_ABI_VERSION = 1
+HEXDYN_ABI_VERSION = 2
 HEXDYN_OK = 0
 HEXDYN_E_ARG = -1
 HEXDYN_E_STATE = -2
@@ -58,7 +58,7 @@ class HexDynDesc(C.Structure):
         ("epssm_minimum", C.c_float), ("epssm_maximum", C.c_float), ("epssm_bottom_z", C.c_float),
         ("epssm_top_z", C.c_float),
         ("rgas", C.c_float), ("cp", C.c_float), ("gravity", C.c_float), ("p0", C.c_float),
-        ("acoustic_dts2", C.c_float * 3),
+        ("acoustic_dts2", C.c_float * 3), ("time_integration_order", C.c_int32),
     ]
 
 

@@ -92,9 +92,11 @@ class DycoreConfig:
     def validate(self) -> None:
         if not math.isfinite(self.config_dt) or self.config_dt <= 0.0:
             _refuse("config_dt", self.config_dt, "the timestep must be finite and positive", "config_dt>0")
-        if self.config_time_integration_order != 3:
+        if (isinstance(self.config_time_integration_order, bool)
+                or self.config_time_integration_order not in (2, 3)):
             _refuse("config_time_integration_order", self.config_time_integration_order,
-                    "the GPU path implements the RK3 schedule only", "config_time_integration_order=3")
+                    "the MPAS split-explicit loop has only order-2 and order-3 schedules",
+                    "config_time_integration_order=2 or 3")
         if not isinstance(self.config_number_of_sub_steps, int) or self.config_number_of_sub_steps < 1:
             _refuse("config_number_of_sub_steps", self.config_number_of_sub_steps,
                     "the split-explicit acoustic loop requires a positive count", "config_number_of_sub_steps>=1")

@@ -47,8 +47,11 @@ def mesh_array(mesh: Any, name: str) -> np.ndarray:
 
 
 def _schedule_dts(cfg: DycoreConfig) -> list[float]:
+    """Acoustic time step of the three RK stages (hexcore/integration.py:104-160)."""
     dt_dyn = cfg.config_dt / cfg.config_dynamics_split_steps
     n = cfg.config_number_of_sub_steps
+    if cfg.config_time_integration_order == 2:
+        return [dt_dyn / n] * 3
     return [dt_dyn / 3.0, dt_dyn / n, dt_dyn / n]
 
 
@@ -448,5 +451,6 @@ def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terra
     desc.rgas, desc.cp, desc.gravity, desc.p0 = 287.0, 1004.5, 9.80616, 100000.0
     for i, dts in enumerate(_schedule_dts(cfg)):
         desc.acoustic_dts2[i] = float(F32(dts) ** 2)
+    desc.time_integration_order = int(cfg.config_time_integration_order)
     sizes = dict(n_cells=ncells, n_edges=nedges, n_vertices=nvert, n_levels=nlev, n_scalars=int(scalars.shape[0]))
     return desc, keep, sizes

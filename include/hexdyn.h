@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define HEXDYN_ABI_VERSION 1
+#define HEXDYN_ABI_VERSION 2
 
 #define HEXDYN_OK 0
 #define HEXDYN_E_ARG (-1)        /* invalid argument or descriptor */
@@ -121,6 +121,9 @@ typedef struct HexDynDesc {
    * dts**2 (NumPy's scalar power, which is powf and not always dts*dts);
    * zero selects dts*dts. */
   float acoustic_dts2[3];
+  /* config_time_integration_order: 3, or 2 (stages dt/2, dt/2, dt with
+   * n/2, n/2, n substeps of dt/n; hexcore/integration.py:104-160); 0 = 3 */
+  int32_t time_integration_order;
 } HexDynDesc;
 
 typedef struct HexDynHandle HexDynHandle;

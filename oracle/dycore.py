@@ -72,14 +72,20 @@ class OracleConfig:
     cp: float = 1004.5
     gravity: float = 9.80616
     p0: float = 100000.0
+    order: int = 3              # config_time_integration_order (2 or 3)
 
 
-def schedule(dt: float, n_sub: int, splits: int):
-    """``RKSchedule.from_mpas`` order 3 (``integration.py:104-160``)."""
+def schedule(dt: float, n_sub: int, splits: int, order: int = 3):
+    """``RKSchedule.from_mpas`` (``integration.py:104-160``), orders 3 and 2."""
     dt_dyn = dt / splits
-    large = (dt_dyn / 3.0, dt_dyn / 2.0, dt_dyn)
-    acoustic = (dt_dyn / 3.0, dt_dyn / n_sub, dt_dyn / n_sub)
-    counts = (1, max(1, n_sub // 2), n_sub)
+    if order == 2:
+        large = (dt_dyn / 2.0, dt_dyn / 2.0, dt_dyn)
+        acoustic = (dt_dyn / n_sub,) * 3
+        counts = (max(1, n_sub // 2), max(1, n_sub // 2), n_sub)
+    else:
+        large = (dt_dyn / 3.0, dt_dyn / 2.0, dt_dyn)
+        acoustic = (dt_dyn / 3.0, dt_dyn / n_sub, dt_dyn / n_sub)
+        counts = (1, max(1, n_sub // 2), n_sub)
     return [(i + 1, large[i], acoustic[i], counts[i]) for i in range(3)]
 
 
@@ -650,7 +656,7 @@ class OracleDycore:
         cfg = self.cfg
         L = g.nlev
         qtot, cqw, cqu = moist
-        stages = schedule(cfg.dt, cfg.n_sub_steps, cfg.split_steps)
+        stages = schedule(cfg.dt, cfg.n_sub_steps, cfg.split_steps, cfg.order)
         saved = state.copy()
         exner_s, theta_s = T1.exner, T1.theta_m
         rp_s, rtp_s = T1.density_perturbation, T1.rho_theta_perturbation
@@ -663,7 +669,7 @@ class OracleDycore:
         euler_ru, tend_rho, euler_rw = self.euler_terms(saved, T1, qtot, cqw, cqu)
         flux_u = flux_w = None
         for stage, large_dt, dts, n_ac in stages:
-            if stage == 2:
+            if stage == 2 and cfg.order == 3:  # driver.py:2894
                 co = self.vertical_coefficients(dts, exner_s, cur_theta, cur_rtp, cqw, qtot)
             rho_edge = HALF * (cur.rho[:, g.c0] + cur.rho[:, g.c1])
             hdiv = self.mass_flux_divergence(cur.rho_u)
@@ -761,7 +767,9 @@ class OracleDycore:
         g = self.g
         L = g.nlev
         step = F32(dt)
-        wn = F32(1.0 / 3.0) if rk_step == 1 else (HALF if rk_step == 2 else ONE)
+        # transport.py:1749-1755
+        wn = (F32(1.0 / (3.0 if self.cfg.order == 3 else 2.0)) if rk_step == 1
+              else (HALF if rk_step == 2 else ONE))
         target = (ONE - wn) * rho_old + wn * rho_new
         out = stage_q.copy()
         for i in range(old.shape[0]):
@@ -867,7 +875,7 @@ class OracleDycore:
         flux_u, flux_w = fu_sum * inv, fw_sum * inv
         if outer.scalars.shape[0] > 0:
             q = outer.scalars.copy()
-            for stage, large_dt, _, _ in schedule(cfg.dt, cfg.n_sub_steps, 1):
+            for stage, large_dt, _, _ in schedule(cfg.dt, cfg.n_sub_steps, 1, cfg.order):
                 if stage == 3 and cfg.monotonic:
                     q = self.advance_scalars_mono(outer.scalars, q, outer.rho, cur.rho, flux_u, flux_w, large_dt)
                 else:

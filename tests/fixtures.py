@@ -34,11 +34,12 @@ def golden_config(fx: dict) -> dict:
     return {"dt": float(fx["config.dt"]), "n_sub_steps": int(fx["config.n_sub_steps"]),
             "monotonic": bool(int(fx.get("config.monotonic", 1))),
             "apvm_upwinding": float(fx.get("config.apvm_upwinding", 0.5)),
-            "xnutr": float(fx.get("config.xnutr", 0.0)), "zd": float(fx.get("config.zd", 22000.0))}
+            "xnutr": float(fx.get("config.xnutr", 0.0)), "zd": float(fx.get("config.zd", 22000.0)),
+            "order": int(fx.get("config.order", 3))}
 
 
 VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1),
-            ("l2_L12_notracers", 2), ("l2_L12_xnutr", 2)]
+            ("l2_L12_notracers", 2), ("l2_L12_xnutr", 2), ("l2_L12_rk2", 2), ("l2_L12_rk2_sub4", 1)]
 
 
 def inputs(fx: dict) -> dict:

@@ -42,14 +42,16 @@ CASES = {
 
 # Configuration variants on the inputs of a base case (outputs only; the
 # fixture names its base): name -> (base, sub steps, monotonic, apvm, steps,
-# scalars kept, xnutr)
+# scalars kept, xnutr, time integration order)
 VARIANTS = {
-    "l2_L12_sub1": ("l2_L12", 1, True, 0.5, 2, None, 0.0),     # one acoustic substep per stage
-    "l2_L12_sub4": ("l2_L12", 4, True, 0.5, 2, None, 0.0),     # (1, 2, 4) substeps
-    "l2_L12_nomono": ("l2_L12", 2, False, 0.5, 2, None, 0.0),  # standard RK3 transport
-    "l2_L12_noapvm": ("l2_L12", 2, True, 0.0, 1, None, 0.0),   # no APVM upwinding
-    "l2_L12_notracers": ("l2_L12", 2, True, 0.5, 2, 0, 0.0),   # no scalars at all
-    "l2_L12_xnutr": ("l2_L12", 2, True, 0.5, 2, None, 0.2),    # implicit w damping above 22 km
+    "l2_L12_sub1": ("l2_L12", 1, True, 0.5, 2, None, 0.0, 3),     # one acoustic substep per stage
+    "l2_L12_sub4": ("l2_L12", 4, True, 0.5, 2, None, 0.0, 3),     # (1, 2, 4) substeps
+    "l2_L12_nomono": ("l2_L12", 2, False, 0.5, 2, None, 0.0, 3),  # standard RK3 transport
+    "l2_L12_noapvm": ("l2_L12", 2, True, 0.0, 1, None, 0.0, 3),   # no APVM upwinding
+    "l2_L12_notracers": ("l2_L12", 2, True, 0.5, 2, 0, 0.0, 3),   # no scalars at all
+    "l2_L12_xnutr": ("l2_L12", 2, True, 0.5, 2, None, 0.2, 3),    # implicit w damping above 22 km
+    "l2_L12_rk2": ("l2_L12", 2, True, 0.5, 2, None, 0.0, 2),      # order-2 schedule, (1, 1, 2) substeps
+    "l2_L12_rk2_sub4": ("l2_L12", 4, True, 0.5, 1, None, 0.0, 2), # order 2, (2, 2, 4) substeps
 }
 
 
@@ -129,16 +131,19 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
             path = HERE / f"step_{name}.npz"
             np.savez_compressed(path, **out)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
-        for vname, (base, vsub, mono, apvm, vsteps, keep, xnutr) in VARIANTS.items():
+        for vname, (base, vsub, mono, apvm, vsteps, keep, xnutr, order) in VARIANTS.items():
             if base != name or (only and vname not in only):
                 continue
             t0 = time.time()
             vcfg = V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=vsub, config_dynamics_split_steps=3,
                                        config_split_dynamics_transport=True, config_monotonic=mono,
                                        config_positive_definite=False, config_coef_3rd_order=0.25,
-                                       config_apvm_upwinding=apvm, config_xnutr=xnutr, config_zd=22000.0)
+                                       config_apvm_upwinding=apvm, config_xnutr=xnutr, config_zd=22000.0,
+                                       config_time_integration_order=order)
             vout = {"base": np.array(base), "config.dt": dt, "config.n_sub_steps": vsub,
                     "config.monotonic": int(mono), "config.apvm_upwinding": apvm}
+            if order != 3:
+                vout["config.order"] = order
             if xnutr:
                 vout["config.xnutr"] = xnutr
                 vout["config.zd"] = 22000.0

@@ -12,7 +12,8 @@ def test_defaults_validate():
 
 @pytest.mark.parametrize("kw,knob", [
     (dict(config_dt=-1.0), "config_dt"),
-    (dict(config_time_integration_order=2), "config_time_integration_order"),
+    (dict(config_time_integration_order=1), "config_time_integration_order"),
+    (dict(config_time_integration_order=4), "config_time_integration_order"),
     (dict(config_dynamics_split_steps=2), "config_dynamics_split_steps"),
     (dict(config_split_dynamics_transport=False), "config_split_dynamics_transport"),
     (dict(config_smdiv=0.0), "config_smdiv"),
@@ -43,3 +44,19 @@ def test_rk3_schedule_matches_mpas():
     assert [s[3] for s in st] == [1, 1, 2]
     st6 = schedule(720.0, 6, 3)
     assert [s[3] for s in st6] == [1, 3, 6]
+
+
+@pytest.mark.parametrize("dt,substeps", [(15.0, 2), (20.0, 4), (60.0, 2)])
+def test_rk2_schedule_matches_mpas(dt, substeps):
+    """tests/test_rk2_v841.py:30-45 of the reference: counts (n/2, n/2, n),
+    and the FP32 large steps equal the FP32 rk_timestep of atm_srk3
+    (order 2 takes the half-step branch at both first stages)."""
+    import numpy as np
+
+    st = schedule(dt, substeps, 3, order=2)
+    assert [s[3] for s in st] == [substeps // 2, substeps // 2, substeps]
+    dyn = np.float32(np.float32(dt) / np.float32(3.0))
+    want = [np.float32(dyn / np.float32(2.0)), np.float32(dyn / np.float32(2.0)), dyn]
+    assert [np.float32(s[1]).tobytes() for s in st] == [w.tobytes() for w in want]
+    assert np.float32(schedule(dt, substeps, 1, order=2)[0][1]) == np.float32(dt * 0.5)
+    DycoreConfig(config_dt=dt, config_time_integration_order=2, config_number_of_sub_steps=substeps).validate()

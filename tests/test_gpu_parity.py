@@ -50,13 +50,14 @@ def test_strict_step_matches_reference_outputs(name, label, steps):
 @pytest.mark.parametrize("name,steps", VARIANTS)
 def test_strict_step_matches_reference_variants(name, steps):
     """One and four acoustic substeps, standard RK3 transport, no APVM, no
-    tracers, implicit w damping: the CUDA step against the reference run with
-    that configuration."""
+    tracers, implicit w damping, the order-2 schedule: the CUDA step against
+    the reference run with that configuration."""
     fx = load_golden(name)
     c = golden_config(fx)
     cfg = DycoreConfig(config_dt=c["dt"], config_number_of_sub_steps=c["n_sub_steps"],
                        config_monotonic=c["monotonic"], config_apvm_upwinding=c["apvm_upwinding"],
-                       config_xnutr=c["xnutr"], config_zd=c["zd"], moist_coefficients="dry")
+                       config_xnutr=c["xnutr"], config_zd=c["zd"], config_time_integration_order=c["order"],
+                       moist_coefficients="dry")
     drv = hexdyn.from_case(case_from_arrays(inputs(fx)), cfg, capture_graph=True)
     for step in range(1, steps + 1):
         res = drv.step()

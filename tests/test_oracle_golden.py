@@ -43,7 +43,7 @@ def test_oracle_matches_reference_variants(name, steps):
         arr["vertical.dss"] = vertical_velocity_damping(arr["vertical.zgrid"], c["xnutr"], c["zd"])
         assert np.count_nonzero(arr["vertical.dss"]) > 0
     orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["n_sub_steps"], monotonic=c["monotonic"],
-                                         apvm_upwinding=c["apvm_upwinding"], moist="dry"))
+                                         apvm_upwinding=c["apvm_upwinding"], moist="dry", order=c["order"]))
     state = State(*(arr[k].copy() for k in STATE))
     side = None
     for step in range(1, steps + 1):

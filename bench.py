@@ -49,6 +49,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--levels", type=int, default=55)
     ap.add_argument("--condensates", type=int, default=5)
     ap.add_argument("--numerics", default="strict", choices=["strict", "fast"])
+    ap.add_argument("--renumber", default="none", choices=["none", "random", "hilbert"],
+                    help="renumber the mesh entities before the run (the builder already numbers them along a "
+                         "Hilbert curve; random scrambles them, hilbert re-orders a scrambled copy)")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
                     help="choose the block size of every kernel by timing before capturing the graph")
@@ -173,7 +176,16 @@ def build_workload(args):
     from hexdyn.mesh import build_mesh
 
     mesh = build_mesh(args.level, lloyd=20, seed=0)
-    return build_case(mesh, n_levels=args.levels, seed=0, n_condensates=args.condensates)
+    case = build_case(mesh, n_levels=args.levels, seed=0, n_condensates=args.condensates)
+    if getattr(args, "renumber", "none") != "none":
+        from hexdyn import reorder
+        from hexdyn.case import case_arrays
+
+        ren = reorder.random_order(case_arrays(case), seed=0)
+        case = reorder.renumber_case(case, ren)
+        if args.renumber == "hilbert":
+            case = reorder.renumber_case(case, reorder.hilbert_order(case_arrays(case)))
+    return case
 
 
 def workload_config(args, case) -> dict:
@@ -188,6 +200,9 @@ def workload_config(args, case) -> dict:
         "numerics": args.numerics, "moist_coefficients": "native",
         "l2": "inputs larger than L2 (per-step working set > 126 MB)",
         "graph": not args.no_graph,
+        "numbering": {"none": "Hilbert curve of the generators (mesh builder)", "random": "random permutation",
+                      "hilbert": "random permutation re-ordered by hexdyn.reorder.hilbert_order"}[
+                          getattr(args, "renumber", "none")],
     }
 
 

@@ -820,6 +820,14 @@ int hexdyn_device_field(HexDynHandle* h, int field, void** dev_ptr) {
   return HEXDYN_OK;
 }
 
+int hexdyn_acoustic_field(HexDynHandle* h, int which, void** dev_ptr) {
+  if (!h || !dev_ptr) return fail(HEXDYN_E_ARG, "NULL argument");
+  if (which == HEXDYN_WORK_RU_P) *dev_ptr = h->ctx.w.ru_p;
+  else if (which == HEXDYN_WORK_RW_P) *dev_ptr = h->ctx.w.rw_p;
+  else return fail(HEXDYN_E_ARG, "unknown acoustic field %d", which);
+  return HEXDYN_OK;
+}
+
 int hexdyn_level_stride(HexDynHandle* h) { return h ? h->ctx.geo.S : 0; }
 long long hexdyn_launches_per_step(HexDynHandle* h) { return h ? h->ctx.launches_per_step : 0; }
 size_t hexdyn_device_bytes(HexDynHandle* h) { return h ? h->ctx.device_bytes : 0; }

@@ -81,6 +81,7 @@ EXPORTS = {
     "hexdyn_capture_graph": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hexdyn_profile_steps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
     "hexdyn_device_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "hexdyn_acoustic_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "hexdyn_level_stride": (C.c_int, [C.c_void_p]),
     "hexdyn_launches_per_step": (C.c_longlong, [C.c_void_p]),
     "hexdyn_device_bytes": (C.c_size_t, [C.c_void_p]),

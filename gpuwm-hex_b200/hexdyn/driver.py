@@ -291,6 +291,47 @@ class HexDycoreDriver:
         self.time_seconds += nsteps * self.config.config_dt
         return DeviceStepResult(DeviceAtmosphere(self), self.receipt(nsteps, flag.value))
 
+    def acoustic_words(self) -> dict:
+        """The final acoustic words of the last step as logical device views:
+        ``ru_p`` [L][E] and ``rw_p`` [L+1][C] after the last substep of RK
+        stage 3 of the last dynamics subcycle (the reference's restart words,
+        hexcore/cuda_driver.py:4707-4711).  Valid until the next step."""
+        import torch
+
+        out = {}
+        S = self.level_stride
+        for name, which, n, rows in (("ru_p", 0, self.sizes["n_edges"], self.sizes["n_levels"]),
+                                     ("rw_p", 1, self.sizes["n_cells"], self.sizes["n_levels"] + 1)):
+            ptr = C.c_void_p()
+            _lib.check(self._lib.hexdyn_acoustic_field(self._handle, which, C.byref(ptr)))
+            t = torch.as_tensor(_CudaArray(ptr.value, (n, S), self), device="cuda")
+            out[name] = t[:, :rows].t()
+        return out
+
+    def _step_device_v841(self, physics_tendencies: Any = None, *, physics_stage_callback: Any = None,
+                          physics_post_transport_callback: Any = None, physics_mass_loading_count: Any = None,
+                          acoustic_output_callback: Any = None) -> DeviceStepResult:
+        """One large step with the reference's production signature
+        (hexcore/cuda_driver.py:4854, called by
+        hexcore/mpasphys/runtime_v842.py:2310).  The physics hand-offs are
+        outside this path and refused by name before any launch;
+        ``acoustic_output_callback(ru_p=..., rw_p=...)`` receives the final
+        acoustic words after the step (the reference calls it after RK stage
+        3 of every dynamics subcycle; its last call carries these values)."""
+        for knob, value in (("physics_tendencies", physics_tendencies),
+                            ("physics_stage_callback", physics_stage_callback),
+                            ("physics_post_transport_callback", physics_post_transport_callback),
+                            ("physics_mass_loading_count", physics_mass_loading_count)):
+            if value is not None:
+                from .config import ConfigurationRefusal
+
+                raise ConfigurationRefusal(knob, value, "the physics coupling is not on the dry dycore step path",
+                                           f"{knob}=None")
+        res = self.step_device(1)
+        if acoustic_output_callback is not None:
+            acoustic_output_callback(**self.acoustic_words())
+        return res
+
     def profile(self, nsteps: int = 1) -> dict[str, tuple[int, float]]:
         """Per-kernel launches and total milliseconds over ``nsteps`` eager
         steps, each launch bracketed by CUDA events on the driver's stream."""

@@ -182,6 +182,16 @@ int hexdyn_capture_graph(HexDynHandle* h, void* stream);
 /* Device pointer of a field of the current state ([entity][level] padded
  * layout, level stride from hexdyn_level_stride) for zero-copy consumers. */
 int hexdyn_device_field(HexDynHandle* h, int field, void** dev_ptr);
+
+/* The final acoustic words of the last step: the perturbation momenta
+ * ru_p ([edge][level], L levels) and rw_p ([cell][level], L+1 interfaces)
+ * after the last substep of RK stage 3 of the last dynamics subcycle, in
+ * the padded layout.  They are the restart words the reference hands to its
+ * acoustic_output_callback (hexcore/cuda_driver.py:4707-4711; MPAS
+ * Registry.xml restart stream) and stay valid until the next step. */
+#define HEXDYN_WORK_RU_P 0
+#define HEXDYN_WORK_RW_P 1
+int hexdyn_acoustic_field(HexDynHandle* h, int which, void** dev_ptr);
 int hexdyn_level_stride(HexDynHandle* h);
 long long hexdyn_launches_per_step(HexDynHandle* h);
 size_t hexdyn_device_bytes(HexDynHandle* h);

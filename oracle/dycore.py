@@ -692,6 +692,10 @@ class OracleDycore:
             for small in range(1, n_ac + 1):
                 self.acoustic_substep(st, fo, co, dts, small)
                 self.divergence_damping(st, theta_s, dts)
+            if record is not None and stage == 3:
+                # the acoustic words the reference hands to its
+                # acoustic_output_callback (cuda_driver.py:4707-4711)
+                record.append(dict(ru_p=st["ru_p"].copy(), rw_p=st["rw_p"].copy()))
             cand_rp = rp_s + st["rho_pp"]
             cand_rtp = rtp_s + st["rtheta_pp"]
             cand = State(cand_rp + g.rho_base, cand_rtp + g.rtheta_base,

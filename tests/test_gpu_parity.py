@@ -185,3 +185,41 @@ def test_validation_flag_raises_on_bad_state():
     with pytest.raises(FloatingPointError):
         drv = make_driver(arr, 1800.0, 2, "dry")
         drv.step()
+
+
+def test_acoustic_words_and_reference_step_signature():
+    """_step_device_v841 (the reference's production entry) refuses the
+    physics hand-offs by name and hands acoustic_output_callback the final
+    acoustic words, equal to the oracle's ru_p and rw_p after the last
+    substep of RK stage 3 of the last subcycle."""
+    from hexdyn.config import ConfigurationRefusal
+    from oracle.dycore import OracleConfig, OracleDycore, State
+
+    fx = load_golden("l2_L12")
+    arr = inputs(fx)
+    drv = make_driver(arr, float(fx["config.dt"]), int(fx["config.n_sub_steps"]), "dry", graph=True)
+    for kw in ("physics_stage_callback", "physics_post_transport_callback", "physics_mass_loading_count"):
+        with pytest.raises(ConfigurationRefusal) as err:
+            drv._step_device_v841(**{kw: 1})
+        assert err.value.knob == kw
+    with pytest.raises(ConfigurationRefusal):
+        drv._step_device_v841(object())
+    got = {}
+
+    def keep(ru_p, rw_p):
+        got["ru_p"], got["rw_p"] = ru_p.cpu().numpy(), rw_p.cpu().numpy()
+
+    drv._step_device_v841(acoustic_output_callback=keep)
+    record = []
+    orc = OracleDycore(arr, OracleConfig(dt=float(fx["config.dt"]), n_sub_steps=int(fx["config.n_sub_steps"]),
+                                         moist="dry"))
+    orc.step(State(*(arr[k].copy() for k in STATE)), None, record=record)
+    words = [r for r in record if "ru_p" in r]
+    assert len(words) == 3  # one per dynamics subcycle; the last is the step's
+    assert differing_words(got["ru_p"], words[-1]["ru_p"]) == 0
+    assert differing_words(got["rw_p"], words[-1]["rw_p"]) == 0
+    # the step itself is the reference's
+    state = drv.get_state()[0]
+    for k in STATE:
+        assert differing_words(getattr(state, k), fx[f"dry.step1.{k}"]) == 0, k
+    drv.close()

@@ -73,6 +73,7 @@ class OracleConfig:
     gravity: float = 9.80616
     p0: float = 100000.0
     order: int = 3              # config_time_integration_order (2 or 3)
+    smagorinsky: Any = None     # oracle.mixing.SmagorinskyConfig: 2-D Smagorinsky mixing on
 
 
 def schedule(dt: float, n_sub: int, splits: int, order: int = 3):
@@ -258,6 +259,11 @@ class OracleDycore:
     def __init__(self, arrays: dict[str, Any], cfg: OracleConfig | None = None):
         self.cfg = cfg or OracleConfig()
         self.g = Geometry(arrays, self.cfg)
+        self.smag = None
+        if self.cfg.smagorinsky is not None:
+            from oracle.mixing import SmagorinskyMixing
+
+            self.smag = SmagorinskyMixing(self.g, arrays, self.cfg.smagorinsky, self.cfg.dt)
 
     # ----------------------------------------------------------- recovery
     def exner(self, rho_theta):
@@ -353,7 +359,13 @@ class OracleDycore:
             gpt = (pv_v[:, g.voe[:, 1]] - pv_v[:, g.voe[:, 0]]) * g.inv_dv
             gpn = (pv_c[:, g.c1] - pv_c[:, g.c0]) * g.inv_dc
             pv_edge = pv_edge - scale * (v * gpt + u * gpn)
-        return Diag(ke=ke, pv_edge=pv_edge, v=v, extra={"vorticity": vort, "pv_vertex": pv_v})
+        div = np.zeros((L, g.ncells), dtype=F32)
+        for s in range(g.maxedges):
+            cell = np.flatnonzero(g.deg > s)
+            e = g.eoc[cell, s]
+            div[:, cell] = div[:, cell] + (g.csign[cell, s] * g.dv[e]) * u[:, e]
+        div = div * g.inv_area
+        return Diag(ke=ke, pv_edge=pv_edge, v=v, extra={"vorticity": vort, "pv_vertex": pv_v, "divergence": div})
 
     # ------------------------------------------------------- coefficients
     def moist_coefficients(self, scalars):
@@ -667,6 +679,13 @@ class OracleDycore:
         cur_u, cur_w = T1.normal_velocity.copy(), T1.vertical_velocity.copy()
         cached_v = diag.v
         euler_ru, tend_rho, euler_rw = self.euler_terms(saved, T1, qtot, cqw, cqu)
+        mix_theta = None
+        if self.smag is not None:
+            # driver.py:2826-2880: the mixing of the subcycle's start state,
+            # saved with the Euler terms for all three RK stages
+            euler_ru, euler_rw, mix_theta = self.smag.tendencies(
+                T1.normal_velocity, diag.v, T1.vertical_velocity, theta_s, saved.rho,
+                diag.extra["divergence"], diag.extra["vorticity"], euler_ru, euler_rw)
         flux_u = flux_w = None
         for stage, large_dt, dts, n_ac in stages:
             if stage == 2 and cfg.order == 3:  # driver.py:2894
@@ -677,6 +696,8 @@ class OracleDycore:
             tend_ru = self.momentum(cur_u, rho_edge, diag.pv_edge, diag.ke, hdiv, tend_ru)
             tend_ru = tend_ru + euler_ru
             tend_rt = self.rho_theta_tendency(cur, saved, cur_theta, theta_s, stage)
+            if mix_theta is not None:
+                tend_rt = tend_rt + mix_theta  # driver.py:2967
             tend_rw = self.w_tendency(cur, cur_w)
             tend_rw = tend_rw + euler_rw
             tend_om = self.omega(tend_rw, tend_ru)

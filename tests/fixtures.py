@@ -35,7 +35,10 @@ def golden_config(fx: dict) -> dict:
             "monotonic": bool(int(fx.get("config.monotonic", 1))),
             "apvm_upwinding": float(fx.get("config.apvm_upwinding", 0.5)),
             "xnutr": float(fx.get("config.xnutr", 0.0)), "zd": float(fx.get("config.zd", 22000.0)),
-            "order": int(fx.get("config.order", 3))}
+            "order": int(fx.get("config.order", 3)),
+            "smagorinsky": (None if "config.smagorinsky_coef" not in fx else
+                            (float(fx["config.smagorinsky_coef"]), float(fx["config.visc4_2dsmag"]),
+                             float(fx["config.del4u_div_factor"])))}
 
 
 VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1),

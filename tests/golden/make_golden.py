@@ -54,6 +54,14 @@ VARIANTS = {
     "l2_L12_rk2_sub4": ("l2_L12", 4, True, 0.5, 1, None, 0.0, 2), # order 2, (2, 2, 4) substeps
 }
 
+# 2-D Smagorinsky horizontal mixing (v8.4.1 deformation form,
+# hexcore/mixing_v841.py): name -> (base, steps, coefficient, visc4,
+# del4u_div_factor).  The fixture also stores the reference's deformation
+# weights of the mesh.
+SMAG_VARIANTS = {
+    "l2_L12_smag": ("l2_L12", 2, 0.125, 0.05, 10.0),
+}
+
 
 def _stubs() -> str:
     d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
@@ -106,7 +114,8 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
                 out[f"{label}.step{step}.side.{k}"] = np.asarray(getattr(side, k))
 
     for name, (level, nlev, ncond, dt, nsub, nsteps, native) in CASES.items():
-        if only and name not in only and not any(v[0] == name for k, v in VARIANTS.items() if k in only):
+        if only and name not in only and not any(v[0] == name for k, v in {**VARIANTS, **SMAG_VARIANTS}.items()
+                                                 if k in only):
             continue
         t0 = time.time()
         mesh = build_mesh(level, lloyd=20, seed=0)
@@ -154,6 +163,36 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
                 vcase = dataclasses.replace(case, scalars=case.scalars[:keep].copy())
                 vout["config.n_scalars"] = keep
             run(DryDycoreDriver, mesh, vg, ref, vcfg, ac, tm, wp, vcase, vsteps, "dry", vout)
+            path = HERE / f"step_{vname}.npz"
+            np.savez_compressed(path, **vout)
+            print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
+        for vname, (base, vsteps, smag, visc4, divf) in SMAG_VARIANTS.items():
+            if base != name or (only and vname not in only):
+                continue
+            import os
+
+            from hexcore import numerics
+            from hexcore.mixing_v841 import initialize_deformation_weights_v841
+
+            # the reference's strict geometry (glibc sinf/cosf, correctly
+            # rounded asinf/atan2f), built from its shipped sources into a
+            # temporary cache
+            os.environ.setdefault("HEXCORE_NATIVE_CPU_CACHE", tempfile.mkdtemp(prefix="hexdyn_ref_native_"))
+            numerics.set_mode("strict", source="make_golden")
+            t0 = time.time()
+            # the v8.4.1 deformation weights need the spherical-mesh attributes
+            mesh.attrs = {"on_a_sphere": "YES", "sphere_radius": float(mesh.arrays["sphere_radius"])}
+            vcfg = V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, config_dynamics_split_steps=3,
+                                       config_split_dynamics_transport=True, config_monotonic=True,
+                                       config_positive_definite=False, config_coef_3rd_order=0.25,
+                                       config_apvm_upwinding=0.5, config_horiz_mixing="2d_smagorinsky",
+                                       config_smagorinsky_coef=smag, config_visc4_2dsmag=visc4,
+                                       config_del4u_div_factor=divf, config_len_disp=0.0, config_mpas_cam_coef=0.0)
+            vout = {"base": np.array(base), "config.dt": dt, "config.n_sub_steps": nsub,
+                    "config.smagorinsky_coef": smag, "config.visc4_2dsmag": visc4, "config.del4u_div_factor": divf}
+            w = initialize_deformation_weights_v841(mesh, dtype=np.float32)
+            vout["mix.coef_c2"], vout["mix.coef_s2"], vout["mix.coef_cs"] = w.coef_c2, w.coef_s2, w.coef_cs
+            run(DryDycoreDriver, mesh, vg, ref, vcfg, ac, tm, wp, case, vsteps, "dry", vout)
             path = HERE / f"step_{vname}.npz"
             np.savez_compressed(path, **vout)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")

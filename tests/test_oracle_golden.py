@@ -72,3 +72,34 @@ def test_dry_state_moist_modes_agree():
         outs.append((st, sd))
     for k in STATE:
         assert differing_words(getattr(outs[0][0], k), getattr(outs[1][0], k)) == 0
+
+
+def test_deformation_weights_match_reference():
+    """hexcore/mixing_v841.py:495 deformation weights of the 162-cell mesh,
+    computed by the reference with its strict geometry."""
+    from oracle.mixing import deformation_weights
+
+    fx = load_golden("l2_L12_smag")
+    c2, s2, cs = deformation_weights(inputs(fx))
+    for got, key in ((c2, "mix.coef_c2"), (s2, "mix.coef_s2"), (cs, "mix.coef_cs")):
+        assert differing_words(got, fx[key]) == 0, key
+
+
+def test_smagorinsky_steps_match_reference():
+    """Two steps with 2-D Smagorinsky mixing (coefficient 0.125, visc4 0.05,
+    del4u_div_factor 10, len_disp from nominalMinDc) equal the reference's."""
+    from oracle.mixing import SmagorinskyConfig
+
+    fx = load_golden("l2_L12_smag")
+    c = golden_config(fx)
+    arr = inputs(fx)
+    orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["n_sub_steps"], moist="dry",
+                                         smagorinsky=SmagorinskyConfig(*c["smagorinsky"])))
+    state = State(*(arr[k].copy() for k in STATE))
+    side = None
+    for step in (1, 2):
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(state, k), fx[f"dry.step{step}.{k}"]) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(getattr(side, k), fx[f"dry.step{step}.side.{k}"]) == 0, (step, k)

@@ -77,6 +77,15 @@ struct HexGeo {
   int apvm_on;
   int moist;          // 0 = dry coefficients, 1 = native (all scalars load)
   int winds_zero;     // u_init and v_init are zero at every level
+  // 2-D Smagorinsky mixing (hexcore/mixing_v841.py), when smag_on
+  int smag_on;
+  const float* deform_c2;   // [C][maxE] deformation weights
+  const float* deform_s2;
+  const float* deform_cs;
+  const float* mix_del2;    // [E] meshScalingDel2
+  const float* mix_del4;    // [E] meshScalingDel4
+  const float* inv_dv_lim;  // [E] min(1/dvEdge, 4/dcEdge)
+  float smag_strain_scale, smag_ceiling, smag_h4, smag_div_factor;
 };
 
 #define HEX_FLAG_DENSITY 1

@@ -116,7 +116,7 @@ __device__ __forceinline__ Win win(const float* __restrict__ col, int k0, int S)
 // hexcore/diagnostics.py:95 compute_solve_diagnostics, v8.4.1 stored inverses.
 
 __global__ void HEX_VEC_BOUNDS kv_diag_vertex(HexGeo g, const float* __restrict__ u, float* __restrict__ pv_vertex,
-                               float* __restrict__ ke_vertex) {
+                               float* __restrict__ ke_vertex, float* __restrict__ vorticity) {
   HEX_VEC_PARALLEL(g.nV)
   const int v = ent, S = g.S;
   V4 vort = v4zero(), ke[3];
@@ -133,25 +133,27 @@ __global__ void HEX_VEC_BOUNDS kv_diag_vertex(HexGeo g, const float* __restrict_
     }
   }
   const float ia = g.inv_area_tri[v], r = 0.25f * g.inv_area_tri[v], f = g.f_vertex[v];
-  V4 pv, kv;
+  V4 pv, kv, vo;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    pv.a[j] = f + vort.a[j] * ia;
+    vo.a[j] = vort.a[j] * ia;
+    pv.a[j] = f + vo.a[j];
     kv.a[j] = (ke[0].a[j] + ke[1].a[j] + ke[2].a[j]) * r;
   }
   st4m(pv_vertex + v * S + k0, pv, k0, 0, g.L);
   st4m(ke_vertex + v * S + k0, kv, k0, 0, g.L);
+  if (vorticity) st4m(vorticity + v * S + k0, vo, k0, 0, g.L);  // the mixing's input
 }
 
 // Cell kinetic energy (v8.4.1 kite blend 0.625) and, with APVM, cell PV.
 __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
                              const float* __restrict__ ke_vertex, float* __restrict__ ke_out,
-                             float* __restrict__ pv_cell) {
+                             float* __restrict__ pv_cell, float* __restrict__ divergence) {
   HEX_VEC_PARALLEL(g.nC)
   const int c = ent, S = g.S;
   const int n = g.deg[c];
   const float ia = g.inv_area[c];
-  V4 ke = v4zero();
+  V4 ke = v4zero(), dv = v4zero();
   HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
@@ -159,6 +161,16 @@ __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ 
     const V4 ue = ld4(u + e * S + k0);
 #pragma unroll
     for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] + 0.25f * (dd * (ue.a[j] * ue.a[j]));
+    if (divergence) {
+      const float sd = g.csign[c * g.maxE + s] * g.dv[e];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dv.a[j] = dv.a[j] + sd * ue.a[j];
+    }
+  }
+  if (divergence) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dv.a[j] = dv.a[j] * ia;
+    st4m(divergence + c * S + k0, dv, k0, 0, g.L);  // the mixing's input
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] * ia * 0.625f;
@@ -460,7 +472,7 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
                              const float* __restrict__ w, const float* __restrict__ edge_theta,
                              const float* __restrict__ edge_w, const float* __restrict__ euler_rw,
                              const float* __restrict__ tend_ru, float* __restrict__ tend_rt,
-                             float* __restrict__ tend_rw, int rk_step) {
+                             float* __restrict__ tend_rw, int rk_step, const float* __restrict__ mix_theta) {
   HEX_VEC_PARALLEL(g.nC)
   const int c = ent, S = g.S, L = g.L;
   const int n = g.deg[c];
@@ -550,8 +562,224 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
     if (k >= 1 && k < L) trw.a[j] = trw.a[j] * (g.fzm[k] * zzw(j) + g.fzp[k] * zzw(j - 1));
     if (k > L) trw.a[j] = 0.0f;
   }
+  if (mix_theta) {
+    // hexcore/driver.py:2967: the saved horizontal theta mixing
+    const V4 mt = ld4(mix_theta + c * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) trt.a[j] = trt.a[j] + mt.a[j];
+  }
   st4m(tend_rt + c * S + k0, trt, k0, 0, g.L);
   st4m(tend_rw + c * S + k0, trw, k0, 0, g.L + 1);
+}
+
+// ------------------------------------------------- horizontal mixing
+// 2-D Smagorinsky mixing of the dynamics subcycle's start state
+// (hexcore/driver.py:2826-2880), v8.4.1 stored-inverse arithmetic.
+
+// NumPy minimum: NaN if either operand is NaN, else the smaller.
+__device__ __forceinline__ float np_min(float a, float b) { return a != a ? a : (b != b ? b : (b < a ? b : a)); }
+
+// hexcore/mixing_v841.py:615 smagorinsky_2d: kdiff of every cell level from
+// the deformation of the edge normal (u) and tangential (v) velocities.
+__global__ void HEX_VEC_BOUNDS kv_smag_kdiff(HexGeo g, const float* __restrict__ u, const float* __restrict__ v,
+                              float* __restrict__ kdiff) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const int n = g.deg[c];
+  V4 dudx = v4zero(), dudy = v4zero(), dvdx = v4zero(), dvdy = v4zero();
+  HEX_GATHER
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float c2 = g.deform_c2[c * g.maxE + s], s2 = g.deform_s2[c * g.maxE + s];
+    const float ccs = g.deform_cs[c * g.maxE + s];
+    const V4 ue = ld4(u + e * S + k0), ve = ld4(v + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      dudx.a[j] = (dudx.a[j] + c2 * ue.a[j]) - ccs * ve.a[j];
+      dudy.a[j] = (dudy.a[j] + ccs * ue.a[j]) - s2 * ve.a[j];
+      dvdx.a[j] = (dvdx.a[j] + ccs * ue.a[j]) + c2 * ve.a[j];
+      dvdy.a[j] = (dvdy.a[j] + s2 * ue.a[j]) + ccs * ve.a[j];
+    }
+  }
+  V4 kd;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float d11 = 2.0f * dudx.a[j], d22 = 2.0f * dvdy.a[j], d12 = dudy.a[j] + dvdx.a[j];
+    const float diff = d11 - d22;
+    const float strain = sqrtf(0.25f * (diff * diff) + d12 * d12);
+    kd.a[j] = np_min(g.smag_strain_scale * strain, g.smag_ceiling);
+  }
+  st4m(kdiff + c * S + k0, kd, k0, 0, g.L);
+}
+
+// hexcore/mixing.py:391-474 second-order momentum filter: delsq_u and the
+// Euler u term plus rho_edge kdiff delsq_u meshScalingDel2 (rho_edge the
+// diagnostics' h_edge of the subcycle's start density).
+__global__ void HEX_VEC_BOUNDS kv_mix_edge2(HexGeo g, const float* __restrict__ div, const float* __restrict__ vort,
+                             const float* __restrict__ kdiff, const float* __restrict__ rho,
+                             const float* __restrict__ euler_ru, float* __restrict__ delsq_u,
+                             float* __restrict__ mix_u) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  const int j0 = g.voe[2 * e] * S + k0, j1 = g.voe[2 * e + 1] * S + k0;
+  const V4 d0 = ld4(div + i0), d1 = ld4(div + i1), z0 = ld4(vort + j0), z1 = ld4(vort + j1);
+  const V4 k0v = ld4(kdiff + i0), k1v = ld4(kdiff + i1), r0 = ld4(rho + i0), r1 = ld4(rho + i1);
+  const V4 eu = ld4(euler_ru + e * S + k0);
+  const float idc = g.inv_dc[e], idv = g.inv_dv_lim[e], del2 = g.mix_del2[e];
+  V4 dq, mu;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float diffusion = (d1.a[j] - d0.a[j]) * idc - (z1.a[j] - z0.a[j]) * idv;
+    dq.a[j] = 0.0f + diffusion;
+    const float h = 0.5f * (r0.a[j] + r1.a[j]);
+    const float kdu = 0.5f * (k0v.a[j] + k1v.a[j]);
+    mu.a[j] = eu.a[j] + h * kdu * diffusion * del2;
+  }
+  st4m(delsq_u + e * S + k0, dq, k0, 0, g.L);
+  st4m(mix_u + e * S + k0, mu, k0, 0, g.L);
+}
+
+// hexcore/mixing.py:533 (w, interfaces 1..L-1) and :638 (theta) second-order
+// filters of a cell, with their Laplacians delsq_w and delsq_theta.
+__global__ void HEX_VEC_BOUNDS kv_mix_cell2(HexGeo g, const float* __restrict__ kdiff, const float* __restrict__ rho,
+                             const float* __restrict__ w, const float* __restrict__ theta,
+                             float* __restrict__ w_mix, float* __restrict__ delsq_w,
+                             float* __restrict__ theta_mix, float* __restrict__ delsq_theta) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  const int n = g.deg[c];
+  const float ia = g.inv_area[c];
+  V4 tw = v4zero(), dw = v4zero(), tt = v4zero(), dt = v4zero();
+  HEX_GATHER
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+    const float sg = g.csign[c * g.maxE + s];
+    const float del2 = g.mix_del2[e];
+    const float esw = 0.5f * ia * sg * g.dv[e] * g.inv_dc[e];
+    const float est = ia * sg * g.dv[e] * g.inv_dc[e];
+    const V4 r0 = ld4(rho + c0 * S + k0), r1 = ld4(rho + c1 * S + k0);
+    const V4 kd0 = ld4(kdiff + c0 * S + k0), kd1 = ld4(kdiff + c1 * S + k0);
+    const V4 w0 = ld4(w + c0 * S + k0), w1 = ld4(w + c1 * S + k0);
+    const V4 t0 = ld4(theta + c0 * S + k0), t1 = ld4(theta + c1 * S + k0);
+    // level k0-1 of rho and kdiff (for the interface below the chunk)
+    const float rm0 = k0 > 0 ? rho[c0 * S + k0 - 1] : 0.0f, rm1 = k0 > 0 ? rho[c1 * S + k0 - 1] : 0.0f;
+    const float km0 = k0 > 0 ? kdiff[c0 * S + k0 - 1] : 0.0f, km1 = k0 > 0 ? kdiff[c1 * S + k0 - 1] : 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      const float h = 0.5f * (r0.a[j] + r1.a[j]);
+      if (k >= 1 && k < L) {
+        const float hm = j == 0 ? 0.5f * (rm0 + rm1) : 0.5f * (r0.a[j - 1] + r1.a[j - 1]);
+        const float kdm0 = j == 0 ? km0 : kd0.a[j - 1], kdm1 = j == 0 ? km1 : kd1.a[j - 1];
+        const float flux = esw * (h + hm) * (w1.a[j] - w0.a[j]);
+        dw.a[j] = dw.a[j] + flux;
+        const float sum_k = kd0.a[j] + kd1.a[j] + kdm0 + kdm1;
+        tw.a[j] = tw.a[j] + flux * del2 * 0.25f * sum_k;
+      }
+      const float ft = est * (t1.a[j] - t0.a[j]) * h;
+      dt.a[j] = dt.a[j] + ft;
+      tt.a[j] = tt.a[j] + ft * 0.5f * (kd0.a[j] + kd1.a[j]) * del2;
+    }
+  }
+  st4m(w_mix + c * S + k0, tw, k0, 0, L + 1);
+  st4m(delsq_w + c * S + k0, dw, k0, 0, L + 1);
+  st4m(theta_mix + c * S + k0, tt, k0, 0, L);
+  st4m(delsq_theta + c * S + k0, dt, k0, 0, L);
+}
+
+// hexcore/mixing.py:464-476: the Laplacians of delsq_u at vertices
+// (vorticity form) and cells (divergence form).
+__global__ void HEX_VEC_BOUNDS kv_mix_lap_vertex(HexGeo g, const float* __restrict__ delsq_u,
+                                  float* __restrict__ delsq_vort) {
+  HEX_VEC_PARALLEL(g.nV)
+  const int v = ent, S = g.S;
+  V4 acc = v4zero();
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int e = g.eov[3 * v + s];
+    const float factor = g.inv_area_tri[v] * g.dc[e] * g.vsign[3 * v + s];
+    const V4 d = ld4(delsq_u + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] + factor * d.a[j];
+  }
+  st4m(delsq_vort + v * S + k0, acc, k0, 0, g.L);
+}
+__global__ void HEX_VEC_BOUNDS kv_mix_lap_cell(HexGeo g, const float* __restrict__ delsq_u,
+                                float* __restrict__ delsq_div) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const int n = g.deg[c];
+  V4 acc = v4zero();
+  HEX_GATHER
+  for (int s = 0; s < n; ++s) {
+    const int e = g.eoc[c * g.maxE + s];
+    const float factor = g.inv_area[c] * g.dv[e] * g.csign[c * g.maxE + s];
+    const V4 d = ld4(delsq_u + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] + factor * d.a[j];
+  }
+  st4m(delsq_div + c * S + k0, acc, k0, 0, g.L);
+}
+
+// hexcore/mixing.py:478-490 fourth-order momentum filter (subtracted).
+__global__ void HEX_VEC_BOUNDS kv_mix_edge4(HexGeo g, const float* __restrict__ rho,
+                             const float* __restrict__ delsq_div, const float* __restrict__ delsq_vort,
+                             float* __restrict__ mix_u) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  const int j0 = g.voe[2 * e] * S + k0, j1 = g.voe[2 * e + 1] * S + k0;
+  const V4 d0 = ld4(delsq_div + i0), d1 = ld4(delsq_div + i1);
+  const V4 z0 = ld4(delsq_vort + j0), z1 = ld4(delsq_vort + j1);
+  const V4 r0 = ld4(rho + i0), r1 = ld4(rho + i1);
+  const float scale = g.mix_del4[e] * g.smag_h4;
+  const float r_dc = scale * g.smag_div_factor * g.inv_dc[e];
+  const float r_dv = scale * g.inv_dv_lim[e];
+  V4 mu = ld4rw(mix_u + e * S + k0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float h = 0.5f * (r0.a[j] + r1.a[j]);
+    const float diffusion = h * ((d1.a[j] - d0.a[j]) * r_dc - (z1.a[j] - z0.a[j]) * r_dv);
+    mu.a[j] = mu.a[j] - diffusion;
+  }
+  st4m(mix_u + e * S + k0, mu, k0, 0, g.L);
+}
+
+// hexcore/mixing.py:576-590 and :719-733 fourth-order w and theta filters
+// (when visc4 > 0), then the saved w term euler_rw + w filter (driver.py:2870).
+__global__ void HEX_VEC_BOUNDS kv_mix_cell4(HexGeo g, const float* __restrict__ delsq_w,
+                             const float* __restrict__ delsq_theta, const float* __restrict__ euler_rw,
+                             const float* __restrict__ w_mix, float* __restrict__ theta_mix,
+                             float* __restrict__ mix_w) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S, L = g.L;
+  V4 tw = ld4(w_mix + c * S + k0), tt = ld4rw(theta_mix + c * S + k0);
+  if (g.smag_h4 > 0.0f) {
+    const int n = g.deg[c];
+    const float scale = g.smag_h4 * g.inv_area[c];
+    HEX_GATHER
+    for (int s = 0; s < n; ++s) {
+      const int e = g.eoc[c * g.maxE + s];
+      const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
+      const float es = g.mix_del4[e] * scale * g.dv[e] * g.csign[c * g.maxE + s] * g.inv_dc[e];
+      const V4 w0 = ld4(delsq_w + c0 * S + k0), w1 = ld4(delsq_w + c1 * S + k0);
+      const V4 t0 = ld4(delsq_theta + c0 * S + k0), t1 = ld4(delsq_theta + c1 * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        if (k >= 1 && k < L) tw.a[j] = tw.a[j] - es * (w1.a[j] - w0.a[j]);
+        tt.a[j] = tt.a[j] - es * (t1.a[j] - t0.a[j]);
+      }
+    }
+  }
+  const V4 er = ld4(euler_rw + c * S + k0);
+  V4 mw;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) mw.a[j] = er.a[j] + tw.a[j];
+  st4m(theta_mix + c * S + k0, tt, k0, 0, L);
+  st4m(mix_w + c * S + k0, mw, k0, 0, L + 1);
 }
 
 // ------------------------------------------------------------- acoustic

@@ -124,8 +124,10 @@ static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexCtx& c = L.ctx;
   const HexGeo& g = c.geo;
   HexWork& w = c.w;
-  LPS(L, g.nV, 1, diag_vertex, g, u, w.pv_vertex, w.ke_vertex);
-  LPS(L, g.nC, 1, diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell);
+  // (vorticity and divergence are kept only for the horizontal mixing)
+  LPS(L, g.nV, 1, diag_vertex, g, u, w.pv_vertex, w.ke_vertex, w.vorticity);
+  LPS(L, g.nC, 1, diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell,
+      w.divergence);
   LPSN(L, recompute_v ? "k_diag_edge_v" : "k_diag_edge", g.nE, 1, diag_edge, g, u, (const float*)w.pv_vertex,
        (const float*)w.pv_cell, w.v, w.pv_edge, recompute_v);
 }
@@ -190,6 +192,26 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
          (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
          w.tend_rho, w.euler_rw);
     L.join();
+    if (g.smag_on) {
+      // 2-D Smagorinsky mixing of the subcycle's start state, saved with the
+      // Euler terms for its three RK stages (hexcore/driver.py:2826-2880)
+      LPS(L, g.nC, 1, smag_kdiff, g, (const float*)s_in->u, (const float*)w.v, w.kdiff);
+      LPS(L, g.nE, 1, mix_edge2, g, (const float*)w.divergence, (const float*)w.vorticity, (const float*)w.kdiff,
+          (const float*)saved->rho, (const float*)w.euler_ru, w.delsq_u, w.mix_u);
+      LPS(L, g.nC, 1, mix_cell2, g, (const float*)w.kdiff, (const float*)saved->rho, (const float*)s_in->w,
+          (const float*)s_in->theta_m, w.w_mix, w.delsq_w, w.theta_mix, w.delsq_theta);
+      if (g.smag_h4 > 0.0f) {
+        LPS(L, g.nV, 1, mix_lap_vertex, g, (const float*)w.delsq_u, w.delsq_vort);
+        LPS(L, g.nC, 1, mix_lap_cell, g, (const float*)w.delsq_u, w.delsq_div);
+        LPS(L, g.nE, 1, mix_edge4, g, (const float*)saved->rho, (const float*)w.delsq_div,
+            (const float*)w.delsq_vort, w.mix_u);
+      }
+      LPS(L, g.nC, 1, mix_cell4, g, (const float*)w.delsq_w, (const float*)w.delsq_theta, (const float*)w.euler_rw,
+          (const float*)w.w_mix, w.theta_mix, w.mix_w);
+    }
+    const float* saved_ru = g.smag_on ? w.mix_u : w.euler_ru;
+    const float* saved_rw = g.smag_on ? w.mix_w : w.euler_rw;
+    const float* saved_theta = g.smag_on ? w.theta_mix : nullptr;
 
     const HexState* cur = saved;
     const HexSide* cs = s_in;
@@ -207,7 +229,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
            w.edge_theta, w.edge_w);
       L.side();
       LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
-           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, (const float*)w.euler_ru, w.tend_ru);
+           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, saved_ru, w.tend_ru);
       if (stg.stage == 2 && ctx.order == 3) {  // hexcore/driver.py:2894
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
@@ -217,7 +239,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       LPS(L, g.nC, 1, tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
            (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
-           (const float*)w.euler_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage);
+           saved_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage, saved_theta);
       // acoustic substeps
       const float inv_dts = 1.0f / dts;
       const float dts2 = stg.dts2;

@@ -251,6 +251,15 @@ int validate(const HexDynDesc* d) {
   if (!(d->smdiv >= 0.0f)) return fail(HEXDYN_E_ARG, "config_smdiv must be non-negative");
   if (!(d->coef_3rd_order >= 0.0f)) return fail(HEXDYN_E_ARG, "config_coef_3rd_order must be non-negative");
   if (!(d->apvm_upwinding >= 0.0f)) return fail(HEXDYN_E_ARG, "config_apvm_upwinding must be non-negative");
+  if (d->horiz_mixing != 0 && d->horiz_mixing != 1)
+    return fail(HEXDYN_E_ARG, "horiz_mixing=%d must be 0 (off) or 1 (2-D Smagorinsky)", d->horiz_mixing);
+  if (d->horiz_mixing) {
+    if (!d->deform_c2 || !d->deform_s2 || !d->deform_cs || !d->mix_del2 || !d->mix_del4)
+      return fail(HEXDYN_E_ARG, "2-D Smagorinsky mixing needs the deformation weights and mesh scalings");
+    if (!(d->smag_strain_scale >= 0.0f) || !(d->smag_ceiling >= 0.0f) || !(d->smag_h4 >= 0.0f) ||
+        !(d->smag_div_factor > 0.0f))
+      return fail(HEXDYN_E_ARG, "invalid Smagorinsky constants");
+  }
   const void* ptrs[] = {d->cells_on_edge, d->edges_on_cell, d->cells_on_cell, d->vertices_on_cell,
                         d->n_edges_on_cell, d->vertices_on_edge, d->edges_on_vertex, d->cells_on_vertex,
                         d->edges_on_edge, d->n_edges_on_edge, d->adv_cells, d->n_adv_cells, d->dc_edge,
@@ -422,6 +431,33 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
     if ((e = upload(c, &g.smdiv_edge, sm)) != cudaSuccess) return cuda_fail(e, "upload smdiv_edge");
   }
   g.moist = d.moist;
+  g.smag_on = d.horiz_mixing ? 1 : 0;
+  if (g.smag_on) {
+    // hexcore/mixing_v841.py:495 weights, hexcore/mixing.py:271 scalings and
+    // the limited inverse dvEdge of hexcore/mixing.py:440
+    std::vector<float> tmp;
+    const size_t slots = (size_t)nC * g.maxE;
+    tmp.assign(d.deform_c2, d.deform_c2 + slots);
+    if ((e = upload(c, &g.deform_c2, tmp)) != cudaSuccess) return cuda_fail(e, "upload deform_c2");
+    tmp.assign(d.deform_s2, d.deform_s2 + slots);
+    if ((e = upload(c, &g.deform_s2, tmp)) != cudaSuccess) return cuda_fail(e, "upload deform_s2");
+    tmp.assign(d.deform_cs, d.deform_cs + slots);
+    if ((e = upload(c, &g.deform_cs, tmp)) != cudaSuccess) return cuda_fail(e, "upload deform_cs");
+    tmp.assign(d.mix_del2, d.mix_del2 + nE);
+    if ((e = upload(c, &g.mix_del2, tmp)) != cudaSuccess) return cuda_fail(e, "upload mix_del2");
+    tmp.assign(d.mix_del4, d.mix_del4 + nE);
+    if ((e = upload(c, &g.mix_del4, tmp)) != cudaSuccess) return cuda_fail(e, "upload mix_del4");
+    tmp.resize(nE);
+    for (int ei = 0; ei < nE; ++ei) {
+      const float idv = 1.0f / d.dv_edge[ei], lim = 4.0f * (1.0f / d.dc_edge[ei]);
+      tmp[ei] = idv < lim ? idv : lim;
+    }
+    if ((e = upload(c, &g.inv_dv_lim, tmp)) != cudaSuccess) return cuda_fail(e, "upload inv_dv_lim");
+    g.smag_strain_scale = d.smag_strain_scale;
+    g.smag_ceiling = d.smag_ceiling;
+    g.smag_h4 = d.smag_h4;
+    g.smag_div_factor = d.smag_div_factor;
+  }
   g.winds_zero = 1;
   for (int k = 0; k < L; ++k)
     if (d.u_init[k] != 0.0f || d.v_init[k] != 0.0f) g.winds_zero = 0;
@@ -467,6 +503,14 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
   for (auto& b : bufs)
     if ((e = dev_alloc(c, b.p, b.n))) return cuda_fail(e, "alloc work");
   if ((e = dev_alloc(c, &w.flag, 1))) return cuda_fail(e, "alloc flag");
+  if (c.geo.smag_on) {
+    struct { float** p; size_t n; } mix[] = {
+        {&w.vorticity, VS}, {&w.divergence, CS}, {&w.kdiff, CS}, {&w.delsq_u, ES}, {&w.delsq_div, CS},
+        {&w.delsq_vort, VS}, {&w.w_mix, CS}, {&w.delsq_w, CS}, {&w.theta_mix, CS}, {&w.delsq_theta, CS},
+        {&w.mix_u, ES}, {&w.mix_w, CS}};
+    for (auto& b : mix)
+      if ((e = dev_alloc(c, b.p, b.n))) return cuda_fail(e, "alloc mixing");
+  }
   // dry coefficients: qtot = 0, cqw = cqu = 1 (hexcore/driver.py:2573,2787)
   k_fill<<<(unsigned)((CS + 255) / 256), 256>>>(w.cqw, CS, 1.0f);
   k_fill<<<(unsigned)((ES + 255) / 256), 256>>>(w.cqu, ES, 1.0f);
@@ -1117,6 +1161,8 @@ int hexdyn_create_ensemble(const HexDynDesc* members, int n_members, HexDynHandl
   for (int m = 0; m < n_members; ++m) {
     int rc = validate(&members[m]);
     if (rc) return fail(rc, "ensemble member %d: %s", m, g_last_error.c_str());
+    if (members[m].horiz_mixing)
+      return fail(HEXDYN_E_ARG, "ensemble member %d: horizontal mixing is not merged across members", m);
     if (m > 0 && (rc = check_compatible(members[0], members[m], m))) return rc;
   }
   HexDynHandle* h = new HexDynHandle();
@@ -1506,6 +1552,8 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
                                    int* flag_out) {
   if (!h || !in || !out) return fail(HEXDYN_E_ARG, "NULL handle or field set");
   const HexCtx& src = h->ctx;
+  if (src.geo.smag_on)
+    return fail(HEXDYN_E_ARG, "the no-allocation step does not carry the mixing work arrays; use hexdyn_step");
   HexState s_in, s_out;
   HexSide d_in, d_out;
   if (!fields_of(in, src.n_scalars, s_in, d_in) || !fields_of(out, src.n_scalars, s_out, d_out))

@@ -44,6 +44,11 @@ struct HexWork {
   // transport
   float *q_stage[2], *edge_q, *target, *scale_in, *scale_out, *mass, *hres_lim;
   int* flag;            // device validation flag (bit set, see HEX_FLAG_*)
+  // 2-D Smagorinsky mixing (allocated when on): diagnostics of the
+  // subcycle's start, diffusivity, Laplacians and the saved mixed terms
+  float *vorticity = nullptr, *divergence = nullptr, *kdiff = nullptr, *delsq_u = nullptr;
+  float *delsq_div = nullptr, *delsq_vort = nullptr, *w_mix = nullptr, *delsq_w = nullptr;
+  float *theta_mix = nullptr, *delsq_theta = nullptr, *mix_u = nullptr, *mix_w = nullptr;
 };
 
 struct HexProfEvent {   // one profiled launch: kernel name and its bracketing events

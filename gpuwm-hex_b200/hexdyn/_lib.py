@@ -10,7 +10,7 @@ from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libhexdyn.so"
 
-HEXDYN_ABI_VERSION = 2
+HEXDYN_ABI_VERSION = 3
 HEXDYN_OK = 0
 HEXDYN_E_ARG = -1
 HEXDYN_E_STATE = -2
@@ -59,6 +59,9 @@ class HexDynDesc(C.Structure):
         ("epssm_top_z", C.c_float),
         ("rgas", C.c_float), ("cp", C.c_float), ("gravity", C.c_float), ("p0", C.c_float),
         ("acoustic_dts2", C.c_float * 3), ("time_integration_order", C.c_int32),
+        ("horiz_mixing", C.c_int32), ("deform_c2", _F32P), ("deform_s2", _F32P), ("deform_cs", _F32P),
+        ("mix_del2", _F32P), ("mix_del4", _F32P), ("smag_strain_scale", C.c_float), ("smag_ceiling", C.c_float),
+        ("smag_h4", C.c_float), ("smag_div_factor", C.c_float),
     ]
 
 

@@ -57,6 +57,13 @@ class DycoreConfig:
     config_xnutr: float = 0.0
     config_zd: float = 22_000.0
     config_horiz_mixing: str = "off"
+    # 2-D Smagorinsky knobs (hexcore/driver.py:193-201; port-safe defaults:
+    # zero active-only coefficients while mixing is off)
+    config_smagorinsky_coef: float = 0.0
+    config_visc4_2dsmag: float = 0.0
+    config_del4u_div_factor: float = 10.0
+    config_h_ScaleWithMesh: bool = True
+    config_mpas_cam_coef: float = 0.0
     config_moist_physics: bool = False
     config_rayleigh_damp_u: bool = False
     config_apply_lbcs: bool = False
@@ -148,10 +155,30 @@ class DycoreConfig:
         if not math.isfinite(self.config_zd) or self.config_zd <= 0.0:
             _refuse("config_zd", self.config_zd, "v8.4.1 requires a finite positive damping start height",
                     "config_zd>0")
-        if self.config_horiz_mixing not in ("off", "2d_fixed"):
+        if self.config_horiz_mixing not in ("off", "2d_fixed", "2d_smagorinsky"):
             _refuse("config_horiz_mixing", self.config_horiz_mixing,
-                    "Smagorinsky mixing is outside this path (mixing is off in its configurations)",
-                    "config_horiz_mixing='off'")
+                    "the v8.4.1 dycore admits off, zero 2d_fixed and 2d_smagorinsky",
+                    "config_horiz_mixing='off' or '2d_smagorinsky'")
+        # hexcore/mixing_v841.py:71-145 (V841MixingConfig) and driver.py:357-395
+        for knob, low, strict in (("config_smagorinsky_coef", 0.0, False), ("config_visc4_2dsmag", 0.0, False),
+                                  ("config_del4u_div_factor", 0.0, True), ("config_mpas_cam_coef", 0.0, False)):
+            value = float(getattr(self, knob))
+            if not math.isfinite(value) or value < low or (strict and value <= low):
+                _refuse(knob, value, "the value is outside the Registry domain", f"an admitted finite {knob}")
+        if not isinstance(self.config_h_ScaleWithMesh, bool):
+            _refuse("config_h_ScaleWithMesh", self.config_h_ScaleWithMesh, "the Registry option is logical",
+                    "config_h_ScaleWithMesh=True or False")
+        if self.config_horiz_mixing == "2d_smagorinsky":
+            if self.config_mpas_cam_coef != 0.0:
+                _refuse("config_mpas_cam_coef", self.config_mpas_cam_coef,
+                        "the CAM viscosity floor is not built (its CPU authority is the reference's Rust "
+                        "library)", "config_mpas_cam_coef=0.0")
+        else:
+            for knob in ("config_smagorinsky_coef", "config_visc4_2dsmag"):
+                if float(getattr(self, knob)) != 0.0:
+                    _refuse(knob, getattr(self, knob), "this Smagorinsky-only knob is inactive when mixing is "
+                            "off and must not be silently ignored",
+                            f"{knob}=0.0 or config_horiz_mixing='2d_smagorinsky'")
         for knob in ("config_moist_physics", "config_rayleigh_damp_u", "config_apply_lbcs"):
             if getattr(self, knob):
                 _refuse(knob, True, "physics, upper damping and limited-area branches are outside this path",

@@ -493,5 +493,28 @@ def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terra
     for i, dts in enumerate(_schedule_dts(cfg)):
         desc.acoustic_dts2[i] = float(F32(dts) ** 2)
     desc.time_integration_order = int(cfg.config_time_integration_order)
+    if cfg.config_horiz_mixing == "2d_smagorinsky":
+        # hexcore/mixing_v841.py: weights, mesh scalings and smagorinsky_2d
+        # constants on the host; the filter length is config_len_disp or,
+        # when zero, nominalMinDc (hexcore/mixing.py:231)
+        from . import mixing
+
+        length = F32(cfg.config_len_disp) if cfg.config_len_disp > 0.0 else F32(float(nominal[0]))
+        geo = {k: mesh_array(mesh, k) for k in ("nEdgesOnCell", "edgesOnCell", "verticesOnCell", "cellsOnEdge",
+                                                 "xCell", "yCell", "zCell", "xVertex", "yVertex", "zVertex",
+                                                 "meshDensity")}
+        try:
+            geo["sphere_radius"] = mesh_array(mesh, "sphere_radius")
+        except AttributeError:
+            geo["sphere_radius"] = np.asarray(float(getattr(mesh, "attrs")["sphere_radius"]))
+        mix = mixing.setup(geo, cfg, length)
+        for name, arr in (("deform_c2", mix.coef_c2), ("deform_s2", mix.coef_s2), ("deform_cs", mix.coef_cs),
+                          ("mix_del2", mix.del2), ("mix_del4", mix.del4)):
+            arr = np.ascontiguousarray(arr, dtype=F32)
+            keep[name] = arr
+            setattr(desc, name, arr.ctypes.data_as(C.POINTER(C.c_float)))
+        desc.horiz_mixing = 1
+        desc.smag_strain_scale, desc.smag_ceiling = float(mix.strain_scale), float(mix.ceiling)
+        desc.smag_h4, desc.smag_div_factor = float(mix.h4), float(mix.div_factor)
     sizes = dict(n_cells=ncells, n_edges=nedges, n_vertices=nvert, n_levels=nlev, n_scalars=int(scalars.shape[0]))
     return desc, keep, sizes

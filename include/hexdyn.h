@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define HEXDYN_ABI_VERSION 2
+#define HEXDYN_ABI_VERSION 3
 
 #define HEXDYN_OK 0
 #define HEXDYN_E_ARG (-1)        /* invalid argument or descriptor */
@@ -124,6 +124,17 @@ typedef struct HexDynDesc {
   /* config_time_integration_order: 3, or 2 (stages dt/2, dt/2, dt with
    * n/2, n/2, n substeps of dt/n; hexcore/integration.py:104-160); 0 = 3 */
   int32_t time_integration_order;
+  /* 2-D Smagorinsky horizontal mixing, v8.4.1 deformation form
+   * (hexcore/mixing_v841.py, hexcore/mixing.py:391-736; config_horiz_mixing
+   * '2d_smagorinsky'): 0 = off.  The host supplies the deformation weights
+   * of every cell slot (atm_initialize_deformation_weights), the per-edge
+   * mesh scalings meshScalingDel2/Del4 and the FP32 constants of
+   * smagorinsky_2d: (c_s len)^2, the diffusivity ceiling 0.01 len^2 / dt,
+   * the fourth-order viscosity visc4 len^3 and config_del4u_div_factor. */
+  int32_t horiz_mixing;
+  const float *deform_c2, *deform_s2, *deform_cs; /* [C][max_edges] */
+  const float *mix_del2, *mix_del4;                /* [E] */
+  float smag_strain_scale, smag_ceiling, smag_h4, smag_div_factor;
 } HexDynDesc;
 
 typedef struct HexDynHandle HexDynHandle;

@@ -42,7 +42,8 @@ def golden_config(fx: dict) -> dict:
 
 
 VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L12_noapvm", 1),
-            ("l2_L12_notracers", 2), ("l2_L12_xnutr", 2), ("l2_L12_rk2", 2), ("l2_L12_rk2_sub4", 1)]
+            ("l2_L12_notracers", 2), ("l2_L12_xnutr", 2), ("l2_L12_rk2", 2), ("l2_L12_rk2_sub4", 1),
+            ("l2_L12_smag", 2)]
 
 
 def inputs(fx: dict) -> dict:

@@ -28,6 +28,14 @@ def cuda():
     torch.cuda.set_device(0)
 
 
+def smag_knobs(c: dict) -> dict:
+    if not c["smagorinsky"]:
+        return {}
+    coef, visc4, divf = c["smagorinsky"]
+    return dict(config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=coef, config_visc4_2dsmag=visc4,
+                config_del4u_div_factor=divf)
+
+
 def make_driver(arr, dt, nsub, moist, numerics="strict", graph=False):
     case = case_from_arrays(arr)
     cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, moist_coefficients=moist, numerics=numerics)
@@ -50,14 +58,15 @@ def test_strict_step_matches_reference_outputs(name, label, steps):
 @pytest.mark.parametrize("name,steps", VARIANTS)
 def test_strict_step_matches_reference_variants(name, steps):
     """One and four acoustic substeps, standard RK3 transport, no APVM, no
-    tracers, implicit w damping, the order-2 schedule: the CUDA step against
-    the reference run with that configuration."""
+    tracers, implicit w damping, the order-2 schedule, 2-D Smagorinsky
+    mixing: the CUDA step against the reference run with that
+    configuration."""
     fx = load_golden(name)
     c = golden_config(fx)
     cfg = DycoreConfig(config_dt=c["dt"], config_number_of_sub_steps=c["n_sub_steps"],
                        config_monotonic=c["monotonic"], config_apvm_upwinding=c["apvm_upwinding"],
                        config_xnutr=c["xnutr"], config_zd=c["zd"], config_time_integration_order=c["order"],
-                       moist_coefficients="dry")
+                       moist_coefficients="dry", **smag_knobs(c))
     drv = hexdyn.from_case(case_from_arrays(inputs(fx)), cfg, capture_graph=True)
     for step in range(1, steps + 1):
         res = drv.step()

@@ -42,8 +42,12 @@ def test_oracle_matches_reference_variants(name, steps):
 
         arr["vertical.dss"] = vertical_velocity_damping(arr["vertical.zgrid"], c["xnutr"], c["zd"])
         assert np.count_nonzero(arr["vertical.dss"]) > 0
+    from oracle.mixing import SmagorinskyConfig
+
+    smag = SmagorinskyConfig(*c["smagorinsky"]) if c["smagorinsky"] else None
     orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["n_sub_steps"], monotonic=c["monotonic"],
-                                         apvm_upwinding=c["apvm_upwinding"], moist="dry", order=c["order"]))
+                                         apvm_upwinding=c["apvm_upwinding"], moist="dry", order=c["order"],
+                                         smagorinsky=smag))
     state = State(*(arr[k].copy() for k in STATE))
     side = None
     for step in range(1, steps + 1):

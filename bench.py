@@ -49,6 +49,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--levels", type=int, default=55)
     ap.add_argument("--condensates", type=int, default=5)
     ap.add_argument("--numerics", default="strict", choices=["strict", "fast"])
+    ap.add_argument("--smagorinsky", action="store_true",
+                    help="2-D Smagorinsky horizontal mixing on (coefficient 0.125, visc4 0.05); off in the "
+                         "workload's configuration")
     ap.add_argument("--renumber", default="none", choices=["none", "random", "hilbert"],
                     help="renumber the mesh entities before the run (the builder already numbers them along a "
                          "Hilbert curve; random scrambles them, hilbert re-orders a scrambled copy)")
@@ -105,6 +108,14 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_fct_cell1": 5 * tcl + tel + 2 * cl + el + ci + conn_c,
         "k_fct_edge": 3 * tcl + 2 * tel + el + conn_e,
         "k_fct_cell2": 6 * tcl + tel + cl + ci + conn_c,
+        # 2-D Smagorinsky mixing (bench --smagorinsky), once per subcycle
+        "k_smag_kdiff": 2 * el + cl + 3 * C * maxE + conn_c,
+        "k_mix_edge2": 3 * cl + vl + 3 * el + conn_e + E * 2,
+        "k_mix_cell2": 3 * cl + 3 * ci + 2 * cl + conn_c,
+        "k_mix_lap_vertex": el + vl + V * 6,
+        "k_mix_lap_cell": el + cl + conn_c,
+        "k_mix_edge4": 2 * cl + vl + 2 * el + conn_e,
+        "k_mix_cell4": 4 * ci + 3 * cl + conn_c,
     }
     if name not in words:
         return 0
@@ -200,6 +211,7 @@ def workload_config(args, case) -> dict:
         "numerics": args.numerics, "moist_coefficients": "native",
         "l2": "inputs larger than L2 (per-step working set > 126 MB)",
         "graph": not args.no_graph,
+        "horizontal_mixing": "2d_smagorinsky (0.125, visc4 0.05)" if getattr(args, "smagorinsky", False) else "off",
         "numbering": {"none": "Hilbert curve of the generators (mesh builder)", "random": "random permutation",
                       "hilbert": "random permutation re-ordered by hexdyn.reorder.hilbert_order"}[
                           getattr(args, "renumber", "none")],
@@ -405,8 +417,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dist = dist_mod
     dt = LEVEL_DT[args.level]
     case = build_workload(args)
+    mixing = (dict(config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=0.125, config_visc4_2dsmag=0.05)
+              if args.smagorinsky else {})
     cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=2, moist_coefficients="native",
-                       numerics=args.numerics)
+                       numerics=args.numerics, **mixing)
     drv = hexdyn.from_case(case, cfg)
     tuning = drv.autotune(2) if args.autotune == "on" else {}
     if not args.no_graph:

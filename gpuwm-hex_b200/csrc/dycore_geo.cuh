@@ -86,6 +86,13 @@ struct HexGeo {
   const float* mix_del4;    // [E] meshScalingDel4
   const float* inv_dv_lim;  // [E] min(1/dvEdge, 4/dcEdge)
   float smag_strain_scale, smag_ceiling, smag_h4, smag_div_factor;
+  // upper damping (hexcore/native/upper_damping.rs): Rayleigh damping of u
+  // over the top rayleigh_levels levels, CAM floor of kdiff over the top
+  // cam_levels levels (0 = off)
+  int rayleigh_levels;
+  float rayleigh_inverse;
+  int cam_levels;
+  float cam_base;
 };
 
 #define HEX_FLAG_DENSITY 1

@@ -145,7 +145,9 @@ __global__ void HEX_VEC_BOUNDS kv_diag_vertex(HexGeo g, const float* __restrict_
   if (vorticity) st4m(vorticity + v * S + k0, vo, k0, 0, g.L);  // the mixing's input
 }
 
-// Cell kinetic energy (v8.4.1 kite blend 0.625) and, with APVM, cell PV.
+// Cell kinetic energy (v8.4.1 kite blend 0.625) and, with APVM, cell PV;
+// DIV: also the divergence of u (the horizontal mixing's input).
+template <bool DIV>
 __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ u, const float* __restrict__ pv_vertex,
                              const float* __restrict__ ke_vertex, float* __restrict__ ke_out,
                              float* __restrict__ pv_cell, float* __restrict__ divergence) {
@@ -161,13 +163,13 @@ __global__ void HEX_VEC_BOUNDS kv_diag_cell(HexGeo g, const float* __restrict__ 
     const V4 ue = ld4(u + e * S + k0);
 #pragma unroll
     for (int j = 0; j < 4; ++j) ke.a[j] = ke.a[j] + 0.25f * (dd * (ue.a[j] * ue.a[j]));
-    if (divergence) {
+    if (DIV) {
       const float sd = g.csign[c * g.maxE + s] * g.dv[e];
 #pragma unroll
       for (int j = 0; j < 4; ++j) dv.a[j] = dv.a[j] + sd * ue.a[j];
     }
   }
-  if (divergence) {
+  if (DIV) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) dv.a[j] = dv.a[j] * ia;
     st4m(divergence + c * S + k0, dv, k0, 0, g.L);  // the mixing's input
@@ -376,6 +378,9 @@ __device__ __forceinline__ float wduz_win(const HexGeo& g, const Win& uw, const 
 }
 
 // tend_ru: vertical transport + hexcore/dynamics_v841.py:121 momentum + saved Euler.
+// RAYLEIGH: the upper Rayleigh damping of u is compiled in (an instance
+// without it keeps the common path's registers).
+template <bool RAYLEIGH>
 __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
                           const float* __restrict__ rho, const float* __restrict__ pv_edge,
                           const float* __restrict__ ke, const float* __restrict__ hdiv,
@@ -436,7 +441,13 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
     const float rho_edge = 0.5f * (rh0.a[j] + rh1.a[j]);
     float horizontal = rho_edge * (q.a[j] - (ke1.a[j] - ke0.a[j]) * idc);
     horizontal = tv + horizontal;
-    const float res = horizontal - uw(j) * 0.5f * (hd0.a[j] + hd1.a[j]);
+    float res = horizontal - uw(j) * 0.5f * (hd0.a[j] + hd1.a[j]);
+    if (RAYLEIGH && k >= g.L - g.rayleigh_levels && k < g.L) {
+      // Rayleigh damping of u before the saved Euler term
+      // (hexcore/native/upper_damping.rs, mpas_atm_time_integration.F:6610-6627)
+      const float coefficient = (float)(k - (g.L - g.rayleigh_levels) + 1) * g.rayleigh_inverse;
+      res = res - (rho_edge * uw(j)) * coefficient;
+    }
     out.a[j] = res + eu.a[j];
   }
   st4m(tend_ru + e * S + k0, out, k0, 0, g.L);
@@ -608,6 +619,13 @@ __global__ void HEX_VEC_BOUNDS kv_smag_kdiff(HexGeo g, const float* __restrict__
     const float diff = d11 - d22;
     const float strain = sqrtf(0.25f * (diff * diff) + d12 * d12);
     kd.a[j] = np_min(g.smag_strain_scale * strain, g.smag_ceiling);
+    const int k = k0 + j;
+    if (k >= g.L - g.cam_levels && k < g.L) {
+      // CAM floor of the diffusivity (hexcore/native/upper_damping.rs,
+      // mpas_atm_time_integration.F:6401-6403)
+      const float floor_k = g.cam_base * (1.0f - (float)(g.L - 1 - k) / (float)g.cam_levels);
+      kd.a[j] = fmaxf(kd.a[j], floor_k);
+    }
   }
   st4m(kdiff + c * S + k0, kd, k0, 0, g.L);
 }

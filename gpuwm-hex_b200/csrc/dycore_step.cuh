@@ -126,8 +126,8 @@ static void diagnostics(Launcher& L, const float* u, int recompute_v) {
   HexWork& w = c.w;
   // (vorticity and divergence are kept only for the horizontal mixing)
   LPS(L, g.nV, 1, diag_vertex, g, u, w.pv_vertex, w.ke_vertex, w.vorticity);
-  LPS(L, g.nC, 1, diag_cell, g, u, (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell,
-      w.divergence);
+  L.lpv("k_diag_cell", g.nC, 1, w.divergence ? kv_diag_cell<true> : kv_diag_cell<false>, g, u,
+        (const float*)w.pv_vertex, (const float*)w.ke_vertex, w.ke, w.pv_cell, w.divergence);
   LPSN(L, recompute_v ? "k_diag_edge_v" : "k_diag_edge", g.nE, 1, diag_edge, g, u, (const float*)w.pv_vertex,
        (const float*)w.pv_cell, w.v, w.pv_edge, recompute_v);
 }
@@ -228,8 +228,9 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       LPS(L, g.nE, 1, edge_adv, g, (const float*)cur->rho_u, (const float*)cs->theta_m, (const float*)cs->w,
            w.edge_theta, w.edge_w);
       L.side();
-      LPS(L, g.nE, 1, tend_u, g, (const float*)cs->u, (const float*)cur->rho_w, (const float*)cur->rho,
-           (const float*)w.pv_edge, (const float*)w.ke, (const float*)w.hdiv, saved_ru, w.tend_ru);
+      L.lpv("k_tend_u", g.nE, 1, g.rayleigh_levels ? kv_tend_u<true> : kv_tend_u<false>, g, (const float*)cs->u,
+            (const float*)cur->rho_w, (const float*)cur->rho, (const float*)w.pv_edge, (const float*)w.ke,
+            (const float*)w.hdiv, saved_ru, w.tend_ru);
       if (stg.stage == 2 && ctx.order == 3) {  // hexcore/driver.py:2894
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,

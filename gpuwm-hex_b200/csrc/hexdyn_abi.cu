@@ -251,6 +251,12 @@ int validate(const HexDynDesc* d) {
   if (!(d->smdiv >= 0.0f)) return fail(HEXDYN_E_ARG, "config_smdiv must be non-negative");
   if (!(d->coef_3rd_order >= 0.0f)) return fail(HEXDYN_E_ARG, "config_coef_3rd_order must be non-negative");
   if (!(d->apvm_upwinding >= 0.0f)) return fail(HEXDYN_E_ARG, "config_apvm_upwinding must be non-negative");
+  if (d->rayleigh_levels < 0 || d->rayleigh_levels > d->n_levels || d->cam_levels < 0 ||
+      d->cam_levels > d->n_levels)
+    return fail(HEXDYN_E_ARG, "upper damping level counts (%d, %d) must lie in 0..n_levels", d->rayleigh_levels,
+                d->cam_levels);
+  if (d->cam_levels && !d->horiz_mixing)
+    return fail(HEXDYN_E_ARG, "the CAM floor applies to the Smagorinsky diffusivity: mixing must be on");
   if (d->horiz_mixing != 0 && d->horiz_mixing != 1)
     return fail(HEXDYN_E_ARG, "horiz_mixing=%d must be 0 (off) or 1 (2-D Smagorinsky)", d->horiz_mixing);
   if (d->horiz_mixing) {
@@ -458,6 +464,10 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
     g.smag_h4 = d.smag_h4;
     g.smag_div_factor = d.smag_div_factor;
   }
+  g.rayleigh_levels = d.rayleigh_levels;
+  g.rayleigh_inverse = d.rayleigh_inverse;
+  g.cam_levels = d.cam_levels;
+  g.cam_base = d.cam_base;
   g.winds_zero = 1;
   for (int k = 0; k < L; ++k)
     if (d.u_init[k] != 0.0f || d.v_init[k] != 0.0f) g.winds_zero = 0;

@@ -10,7 +10,7 @@ from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libhexdyn.so"
 
-HEXDYN_ABI_VERSION = 3
+HEXDYN_ABI_VERSION = 4
 HEXDYN_OK = 0
 HEXDYN_E_ARG = -1
 HEXDYN_E_STATE = -2
@@ -62,6 +62,8 @@ class HexDynDesc(C.Structure):
         ("horiz_mixing", C.c_int32), ("deform_c2", _F32P), ("deform_s2", _F32P), ("deform_cs", _F32P),
         ("mix_del2", _F32P), ("mix_del4", _F32P), ("smag_strain_scale", C.c_float), ("smag_ceiling", C.c_float),
         ("smag_h4", C.c_float), ("smag_div_factor", C.c_float),
+        ("rayleigh_levels", C.c_int32), ("rayleigh_inverse", C.c_float), ("cam_levels", C.c_int32),
+        ("cam_base", C.c_float),
     ]
 
 

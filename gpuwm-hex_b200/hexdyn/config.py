@@ -64,6 +64,9 @@ class DycoreConfig:
     config_del4u_div_factor: float = 10.0
     config_h_ScaleWithMesh: bool = True
     config_mpas_cam_coef: float = 0.0
+    config_number_cam_damping_levels: int = 4
+    config_number_rayleigh_damp_u_levels: int = 6
+    config_rayleigh_damp_u_timescale_days: float = 5.0
     config_moist_physics: bool = False
     config_rayleigh_damp_u: bool = False
     config_apply_lbcs: bool = False
@@ -168,20 +171,32 @@ class DycoreConfig:
         if not isinstance(self.config_h_ScaleWithMesh, bool):
             _refuse("config_h_ScaleWithMesh", self.config_h_ScaleWithMesh, "the Registry option is logical",
                     "config_h_ScaleWithMesh=True or False")
-        if self.config_horiz_mixing == "2d_smagorinsky":
-            if self.config_mpas_cam_coef != 0.0:
-                _refuse("config_mpas_cam_coef", self.config_mpas_cam_coef,
-                        "the CAM viscosity floor is not built (its CPU authority is the reference's Rust "
-                        "library)", "config_mpas_cam_coef=0.0")
-        else:
+        # hexcore/config_v841.py:694-704 upper-damping knobs
+        for knob in ("config_number_cam_damping_levels", "config_number_rayleigh_damp_u_levels"):
+            value = getattr(self, knob)
+            if type(value) is not int or value < 1:
+                _refuse(knob, value, "the native damping loop requires a positive integer level count",
+                        "a positive integer")
+        days = self.config_rayleigh_damp_u_timescale_days
+        if not math.isfinite(days) or days <= 0:
+            _refuse("config_rayleigh_damp_u_timescale_days", days,
+                    "the Rayleigh coefficient divides by a positive timescale", "a finite positive timescale")
+        if self.config_horiz_mixing != "2d_smagorinsky":
             for knob in ("config_smagorinsky_coef", "config_visc4_2dsmag"):
                 if float(getattr(self, knob)) != 0.0:
                     _refuse(knob, getattr(self, knob), "this Smagorinsky-only knob is inactive when mixing is "
                             "off and must not be silently ignored",
                             f"{knob}=0.0 or config_horiz_mixing='2d_smagorinsky'")
-        for knob in ("config_moist_physics", "config_rayleigh_damp_u", "config_apply_lbcs"):
+        if self.config_horiz_mixing != "2d_smagorinsky" and self.config_mpas_cam_coef != 0.0:
+            _refuse("config_mpas_cam_coef", self.config_mpas_cam_coef,
+                    "the CAM floor bounds the Smagorinsky diffusivity and is inactive when mixing is off",
+                    "config_mpas_cam_coef=0.0 or config_horiz_mixing='2d_smagorinsky'")
+        if not isinstance(self.config_rayleigh_damp_u, bool):
+            _refuse("config_rayleigh_damp_u", self.config_rayleigh_damp_u, "the Registry option is logical",
+                    "config_rayleigh_damp_u=True or False")
+        for knob in ("config_moist_physics", "config_apply_lbcs"):
             if getattr(self, knob):
-                _refuse(knob, True, "physics, upper damping and limited-area branches are outside this path",
+                _refuse(knob, True, "physics and limited-area branches are outside this path",
                         f"{knob}=False")
         if self.moist_coefficients not in ("native", "dry"):
             _refuse("moist_coefficients", self.moist_coefficients, "unknown coefficient semantics",

@@ -516,5 +516,15 @@ def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terra
         desc.horiz_mixing = 1
         desc.smag_strain_scale, desc.smag_ceiling = float(mix.strain_scale), float(mix.ceiling)
         desc.smag_h4, desc.smag_div_factor = float(mix.h4), float(mix.div_factor)
+        if cfg.config_mpas_cam_coef > 0.0:
+            # hexcore/native/upper_damping.rs CAM floor: ((4 x 2.0833) len) coef in FP32
+            desc.cam_levels = int(cfg.config_number_cam_damping_levels)
+            desc.cam_base = float(((F32(4.0) * F32(2.0833)) * length) * F32(cfg.config_mpas_cam_coef))
+    if cfg.config_rayleigh_damp_u:
+        # hexcore/native/upper_damping.rs Rayleigh coefficient base 1/(levels (days 86400)) in FP32
+        levels = int(cfg.config_number_rayleigh_damp_u_levels)
+        days = F32(cfg.config_rayleigh_damp_u_timescale_days)
+        desc.rayleigh_levels = levels
+        desc.rayleigh_inverse = float(F32(1.0) / (F32(levels) * (days * F32(86400.0))))
     sizes = dict(n_cells=ncells, n_edges=nedges, n_vertices=nvert, n_levels=nlev, n_scalars=int(scalars.shape[0]))
     return desc, keep, sizes

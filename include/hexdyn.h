@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define HEXDYN_ABI_VERSION 3
+#define HEXDYN_ABI_VERSION 4
 
 #define HEXDYN_OK 0
 #define HEXDYN_E_ARG (-1)        /* invalid argument or descriptor */
@@ -135,6 +135,16 @@ typedef struct HexDynDesc {
   const float *deform_c2, *deform_s2, *deform_cs; /* [C][max_edges] */
   const float *mix_del2, *mix_del4;                /* [E] */
   float smag_strain_scale, smag_ceiling, smag_h4, smag_div_factor;
+  /* Upper damping (hexcore/native/upper_damping.rs, the reference's native
+   * operators): Rayleigh damping of u over the top rayleigh_levels levels
+   * (0 = off; config_rayleigh_damp_u) with rayleigh_inverse =
+   * 1/(levels (days 86400)) in FP32; the CAM floor of the Smagorinsky
+   * diffusivity over the top cam_levels levels (0 = off;
+   * config_mpas_cam_coef > 0) with cam_base = ((4 x 2.0833) len) coef. */
+  int32_t rayleigh_levels;
+  float rayleigh_inverse;
+  int32_t cam_levels;
+  float cam_base;
 } HexDynDesc;
 
 typedef struct HexDynHandle HexDynHandle;

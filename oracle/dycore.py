@@ -74,6 +74,7 @@ class OracleConfig:
     p0: float = 100000.0
     order: int = 3              # config_time_integration_order (2 or 3)
     smagorinsky: Any = None     # oracle.mixing.SmagorinskyConfig: 2-D Smagorinsky mixing on
+    rayleigh: Any = None        # (levels, days): Rayleigh damping of u over the top levels
 
 
 def schedule(dt: float, n_sub: int, splits: int, order: int = 3):
@@ -694,6 +695,13 @@ class OracleDycore:
             hdiv = self.mass_flux_divergence(cur.rho_u)
             tend_ru = self.vertical_transport_u(cur_u, cur.rho_w)
             tend_ru = self.momentum(cur_u, rho_edge, diag.pv_edge, diag.ke, hdiv, tend_ru)
+            if self.cfg.rayleigh is not None:
+                # Rayleigh damping of u before the saved Euler term
+                # (hexcore/native/upper_damping.rs upper_rayleigh, driver.py:2941)
+                levels, days = self.cfg.rayleigh
+                inv = F32(1.0) / (F32(levels) * (F32(days) * F32(86400.0)))
+                for k in range(L - levels, L):
+                    tend_ru[k] = tend_ru[k] - (rho_edge[k] * cur_u[k]) * (F32(k - (L - levels) + 1) * inv)
             tend_ru = tend_ru + euler_ru
             tend_rt = self.rho_theta_tendency(cur, saved, cur_theta, theta_s, stage)
             if mix_theta is not None:

@@ -157,6 +157,8 @@ class SmagorinskyConfig:
     coef: float = 0.125            # config_smagorinsky_coef
     visc4: float = 0.05            # config_visc4_2dsmag
     del4u_div_factor: float = 10.0  # config_del4u_div_factor
+    cam_coef: float = 0.0           # config_mpas_cam_coef (CAM floor of kdiff when > 0)
+    cam_levels: int = 4             # config_number_cam_damping_levels
 
 
 class SmagorinskyMixing:
@@ -173,6 +175,9 @@ class SmagorinskyMixing:
         self.ceiling = (F32(0.01) * (length * length)) * inv_dt
         self.h4 = F32(cfg.visc4) * ((length * length) * length)
         self.factor4 = F32(cfg.del4u_div_factor)
+        # CAM floor (hexcore/native/upper_damping.rs upper_cam)
+        self.cam_levels = int(cfg.cam_levels) if cfg.cam_coef > 0.0 else 0
+        self.cam_base = ((F32(4.0) * F32(2.0833)) * length) * F32(cfg.cam_coef)
         # meshScalingDel2/Del4 (mixing.py:271, config_h_ScaleWithMesh)
         from oracle.powf import powf_gnu
 
@@ -204,6 +209,10 @@ class SmagorinskyMixing:
             diff = d11 - d22
             strain = np.sqrt(quarter * (diff * diff) + d12 * d12)
             kd[:, cell] = np.minimum(self.strain_scale * strain, self.ceiling)
+        lv = self.cam_levels
+        for k in range(L - lv, L) if lv else ():
+            floor = self.cam_base * (F32(1.0) - F32(L - 1 - k) / F32(lv))
+            kd[k] = np.fmax(kd[k], floor)
         return kd
 
     def tendencies(self, u, v, w, theta, rho, divergence, vorticity, euler_ru, euler_rw):

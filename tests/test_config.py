@@ -21,7 +21,9 @@ def test_defaults_validate():
     (dict(config_xnutr=1.5), "config_xnutr"),
     (dict(config_xnutr=0.2, config_zd=0.0), "config_zd"),
     (dict(config_horiz_mixing="3d_smagorinsky"), "config_horiz_mixing"),
-    (dict(config_horiz_mixing="2d_smagorinsky", config_mpas_cam_coef=0.1), "config_mpas_cam_coef"),
+    (dict(config_mpas_cam_coef=0.1), "config_mpas_cam_coef"),
+    (dict(config_number_rayleigh_damp_u_levels=0), "config_number_rayleigh_damp_u_levels"),
+    (dict(config_rayleigh_damp_u_timescale_days=0.0), "config_rayleigh_damp_u_timescale_days"),
     (dict(config_smagorinsky_coef=0.125), "config_smagorinsky_coef"),
     (dict(config_horiz_mixing="2d_smagorinsky", config_del4u_div_factor=0.0), "config_del4u_div_factor"),
     (dict(config_moist_physics=True), "config_moist_physics"),

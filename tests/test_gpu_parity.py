@@ -232,3 +232,37 @@ def test_acoustic_words_and_reference_step_signature():
     for k in STATE:
         assert differing_words(getattr(state, k), fx[f"dry.step1.{k}"]) == 0, k
     drv.close()
+
+
+def test_upper_damping_matches_oracle():
+    """Rayleigh damping of u over the top 6 levels (5-day timescale) and the
+    CAM floor of the Smagorinsky diffusivity over the top 4 levels: the CUDA
+    step equals the oracle's restatement of the reference's native operators
+    (hexcore/native/upper_damping.rs) word for word over two steps.  (The
+    reference's own CPU path for them needs a Rust toolchain, so this
+    parity is against the restatement only.)"""
+    from oracle.dycore import OracleConfig, OracleDycore, State
+    from oracle.mixing import SmagorinskyConfig
+
+    fx = load_golden("l2_L12")
+    arr = inputs(fx)
+    dt, nsub = float(fx["config.dt"]), int(fx["config.n_sub_steps"])
+    cfg = DycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, moist_coefficients="dry",
+                       config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=0.125,
+                       config_visc4_2dsmag=0.05, config_mpas_cam_coef=2.0, config_rayleigh_damp_u=True)
+    drv = hexdyn.from_case(case_from_arrays(arr), cfg, capture_graph=True)
+    orc = OracleDycore(arr, OracleConfig(dt=dt, n_sub_steps=nsub, moist="dry", rayleigh=(6, 5.0),
+                                         smagorinsky=SmagorinskyConfig(0.125, 0.05, 10.0, cam_coef=2.0)))
+    state, side = State(*(arr[k].copy() for k in STATE)), None
+    plain = fx["dry.step1.rho_u"]
+    for step in (1, 2):
+        res = drv.step()
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), getattr(state, k)) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), getattr(side, k)) == 0, (step, k)
+        if step == 1:
+            # the damping acts: the top levels differ from the undamped step
+            assert differing_words(res.state.rho_u[-6:], plain[-6:]) > 0
+    drv.close()

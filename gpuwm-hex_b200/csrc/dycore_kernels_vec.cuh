@@ -660,7 +660,10 @@ __global__ void HEX_VEC_BOUNDS kv_mix_edge2(HexGeo g, const float* __restrict__ 
 
 // hexcore/mixing.py:533 (w, interfaces 1..L-1) and :638 (theta) second-order
 // filters of a cell, with their Laplacians delsq_w and delsq_theta.
-__global__ void HEX_VEC_BOUNDS kv_mix_cell2(HexGeo g, const float* __restrict__ kdiff, const float* __restrict__ rho,
+#ifndef HEX_MIX_CELL2_MIN_BLOCKS
+#define HEX_MIX_CELL2_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(256, HEX_MIX_CELL2_MIN_BLOCKS) kv_mix_cell2(HexGeo g, const float* __restrict__ kdiff, const float* __restrict__ rho,
                              const float* __restrict__ w, const float* __restrict__ theta,
                              float* __restrict__ w_mix, float* __restrict__ delsq_w,
                              float* __restrict__ theta_mix, float* __restrict__ delsq_theta) {

@@ -119,37 +119,6 @@ __global__ void k_rebuild_cell(HexGeo g, const float* __restrict__ rho, const fl
   }
 }
 
-// --------------------------------------------------- moist coefficients
-// hexcore/regional_v841.py:1180 compute_moist_coefficients, every scalar.
-
-__global__ void k_moist_cell(HexGeo g, const float* __restrict__ q, int nT, float* __restrict__ qtot,
-                             float* __restrict__ cqw) {
-  HEX_LEVEL_PARALLEL(g.nC)
-  if (k >= g.L) return;
-  const int c = ent, S = g.S;
-  auto qt = [&](int kk) {
-    float acc = 0.0f;
-    for (int t = 0; t < nT; ++t) acc = acc + q[((size_t)t * g.nC + c) * S + kk];
-    return acc;
-  };
-  const float here = qt(k);
-  qtot[c * S + k] = here;
-  cqw[c * S + k] = k == 0 ? 1.0f : 1.0f / (1.0f + 0.5f * (here + qt(k - 1)));
-}
-
-__global__ void k_moist_edge(HexGeo g, const float* __restrict__ q, int nT, float* __restrict__ cqu) {
-  HEX_LEVEL_PARALLEL(g.nE)
-  if (k >= g.L) return;
-  const int e = ent, S = g.S;
-  const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
-  float acc = 0.0f;
-  for (int t = 0; t < nT; ++t) {
-    const float* qt = q + (size_t)t * g.nC * S;
-    acc = acc + 0.5f * (qt[c0 * S + k] + qt[c1 * S + k]);
-  }
-  cqu[e * S + k] = 1.0f / (1.0f + acc);
-}
-
 // -------------------------------------------------- vertical coefficients
 // hexcore/acoustic_v841.py:81 compute_vertical_implicit_coefficients_v841.
 __global__ void k_vcoef(HexGeo g, float dts2, const float* __restrict__ exner,

@@ -112,6 +112,56 @@ __device__ __forceinline__ Win win(const float* __restrict__ col, int k0, int S)
   return w;
 }
 
+// --------------------------------------------------- moist coefficients
+// hexcore/regional_v841.py:1180 compute_moist_coefficients, every scalar:
+// qtot = sum of the scalars in scalar order, cqw = 1/(1 + (qtot(k) +
+// qtot(k-1))/2) above the surface, cqu = 1/(1 + sum of the two-cell means).
+// Scalars are stored [scalar][cell][S].
+__global__ void HEX_VEC_BOUNDS kv_moist_cell(HexGeo g, const float* __restrict__ q, int nT,
+                                             float* __restrict__ qtot, float* __restrict__ cqw) {
+  HEX_VEC_PARALLEL(g.nC)
+  const int c = ent, S = g.S;
+  const size_t tstride = (size_t)g.nC * S;
+  const float* qc = q + c * S + k0;
+  V4 acc = v4zero();
+  float below = 0.0f;  // qtot at level k0 - 1
+  HEX_GATHER
+  for (int t = 0; t < nT; ++t) {
+    const V4 v = ld4(qc + t * tstride);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] + v.a[j];
+    if (k0 > 0) below = below + (qc - 1)[t * tstride];
+  }
+  V4 cw;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float prev = j == 0 ? below : acc.a[j - 1];
+    cw.a[j] = k0 + j == 0 ? 1.0f : 1.0f / (1.0f + 0.5f * (acc.a[j] + prev));
+  }
+  st4m(qtot + c * S + k0, acc, k0, 0, g.L);
+  st4m(cqw + c * S + k0, cw, k0, 0, g.L);
+}
+
+__global__ void HEX_VEC_BOUNDS kv_moist_edge(HexGeo g, const float* __restrict__ q, int nT,
+                                             float* __restrict__ cqu) {
+  HEX_VEC_PARALLEL(g.nE)
+  const int e = ent, S = g.S;
+  const size_t tstride = (size_t)g.nC * S;
+  const float* q0 = q + g.coe[2 * e] * S + k0;
+  const float* q1 = q + g.coe[2 * e + 1] * S + k0;
+  V4 acc = v4zero();
+  HEX_GATHER
+  for (int t = 0; t < nT; ++t) {
+    const V4 a = ld4(q0 + t * tstride), b = ld4(q1 + t * tstride);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc.a[j] = acc.a[j] + 0.5f * (a.a[j] + b.a[j]);
+  }
+  V4 out;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) out.a[j] = 1.0f / (1.0f + acc.a[j]);
+  st4m(cqu + e * S + k0, out, k0, 0, g.L);
+}
+
 // ---------------------------------------------------------- diagnostics
 // hexcore/diagnostics.py:95 compute_solve_diagnostics, v8.4.1 stored inverses.
 
@@ -1227,6 +1277,12 @@ __device__ __forceinline__ float fct_vres_win(const HexGeo& g, float step, const
 
 // hexcore/transport.py:1919-2118 (v8.4.1 order): bounds, low-order mass,
 // incoming/outgoing antidiffusive totals and the scale factors.
+// ACROSS: cellsOnCell[c][s] is the cell across edgesOnCell[c][s] for every
+// slot (the MPAS convention, checked on the host), so the upwind flux of
+// slot s takes its two cell values from this column and the neighbour column
+// the bounds already load; the min/max over neighbours and the mass sums
+// still run in slot order, so the words are those of the two-loop form.
+template <bool ACROSS>
 __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const float* __restrict__ q_old,
                              const float* __restrict__ q_stage, const float* __restrict__ rho_old,
                              const float* __restrict__ hv, const float* __restrict__ ww,
@@ -1250,13 +1306,15 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
     mx[j] = fmaxf(fmaxf(a, o), b);
   }
   const int n = g.deg[c];
-  HEX_GATHER
-  for (int s = 0; s < n; ++s) {
-    const V4 on = ld4(ot + g.coc[c * g.maxE + s] * S + k0);
+  if (!ACROSS) {
+    HEX_GATHER
+    for (int s = 0; s < n; ++s) {
+      const V4 on = ld4(ot + g.coc[c * g.maxE + s] * S + k0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      mn[j] = pymin(mn[j], on.a[j] + 0.0f);
-      mx[j] = pymax(mx[j], on.a[j] + 0.0f);
+      for (int j = 0; j < 4; ++j) {
+        mn[j] = pymin(mn[j], on.a[j] + 0.0f);
+        mx[j] = pymax(mx[j], on.a[j] + 0.0f);
+      }
     }
   }
   const V4 ro = ld4(rho_old + ii), td = ld4(target + ii);
@@ -1277,10 +1335,25 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
   HEX_GATHER
   for (int s = 0; s < n; ++s) {
     const int e = g.eoc[c * g.maxE + s];
-    const float ts = -g.csign[c * g.maxE + s];
+    const float cs = g.csign[c * g.maxE + s];
+    const float ts = -cs;
     const float dvs = g.dv[e] * step;
     const V4 vel = ld4(hv + e * S + k0), h = ld4(he + e * S + k0);
-    const V4 o0 = ld4(ot + g.coe[2 * e] * S + k0), o1 = ld4(ot + g.coe[2 * e + 1] * S + k0);
+    V4 o0, o1;
+    if (ACROSS) {
+      // csign > 0: this cell is the edge's first cell
+      const V4 on = ld4(ot + g.coc[c * g.maxE + s] * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        mn[j] = pymin(mn[j], on.a[j] + 0.0f);
+        mx[j] = pymax(mx[j], on.a[j] + 0.0f);
+        o0.a[j] = cs > 0.0f ? ow(j) : on.a[j];
+        o1.a[j] = cs > 0.0f ? on.a[j] : ow(j);
+      }
+    } else {
+      o0 = ld4(ot + g.coe[2 * e] * S + k0);
+      o1 = ld4(ot + g.coe[2 * e + 1] * S + k0);
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const float upw = dvs * (pos0(vel.a[j]) * (o0.a[j] + 0.0f) + neg0(vel.a[j]) * (o1.a[j] + 0.0f));

@@ -160,8 +160,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   const size_t sm_ac_v = sizeof(float) * g.S * HEX_ACV_SMEM_ARRAYS;
 
   if (g.moist) {
-    LP(L, g.nC, 1, 0, k_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
-    LP(L, g.nE, 1, 0, k_moist_edge, g, (const float*)in.scalars, nT, w.cqu);
+    L.lpv("k_moist_cell", g.nC, 1, kv_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);
+    L.lpv("k_moist_edge", g.nE, 1, kv_moist_edge, g, (const float*)in.scalars, nT, w.cqu);
   }
   // initial solve diagnostics with v reconstructed (rk_step=3)
   diagnostics(L, side_in.u, 1);
@@ -315,8 +315,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
              (const float*)w.flux_w, w.target, w.flag);
         L.lpvt("k_tr_edge", g.nE, (nT + HEX_TR_GROUP - 1) / HEX_TR_GROUP, kv_tr_edge, g, nT, 1, q_prev,
                (const float*)w.flux_u, w.edge_q);
-        LPST(L, g.nC, nT, fct_cell1, g, step, (const float*)in.scalars, q_prev, (const float*)in.rho,
-             (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
+        L.lpvt("k_fct_cell1", g.nC, nT, g.coc_across ? kv_fct_cell1<true> : kv_fct_cell1<false>, g, nT, step,
+             (const float*)in.scalars, q_prev, (const float*)in.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass);
         LPST(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);

@@ -353,10 +353,12 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
   std::vector<int> nadv(d.n_adv_cells, d.n_adv_cells + nE);
   std::vector<int> kite_slot((size_t)nC * mE, 0);
   std::vector<float> csign((size_t)nC * mE, 0.0f), vsign(3 * (size_t)nV, 0.0f);
+  g.coc_across = 1;
   for (int ci = 0; ci < nC; ++ci)
     for (int s = 0; s < deg[ci]; ++s) {
       const int e = eoc[(size_t)ci * mE + s];
       csign[(size_t)ci * mE + s] = coe[2 * e] == ci ? 1.0f : -1.0f;         // hexcore/acoustic.py:224
+      if (coc[(size_t)ci * mE + s] != (coe[2 * e] == ci ? coe[2 * e + 1] : coe[2 * e])) g.coc_across = 0;
       const int v = voc[(size_t)ci * mE + s];
       int slot = -1;
       for (int j = 0; j < 3; ++j)

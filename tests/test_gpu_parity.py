@@ -101,6 +101,28 @@ def test_renumbered_case_matches_reference(seed):
     drv.close()
 
 
+def test_cells_on_cell_slot_order_does_not_change_the_step():
+    """The limiter's bounds are a min/max over cellsOnCell.  When its slots
+    follow edgesOnCell (the MPAS convention) the library takes the upwind
+    fluxes' cell values from the columns the bounds load; here the slots are
+    rotated by one, so it gathers them per edge instead, and the words are
+    still the reference's."""
+    fx = load_golden("l2_L12")
+    arr = dict(inputs(fx))
+    coc = arr["mesh.cellsOnCell"].copy()
+    counts = arr["mesh.nEdgesOnCell"]
+    for c in range(coc.shape[0]):
+        m = int(counts[c])
+        coc[c, :m] = np.roll(coc[c, :m], 1)
+    arr["mesh.cellsOnCell"] = coc
+    drv = make_driver(arr, float(fx["config.dt"]), int(fx["config.n_sub_steps"]), "dry")
+    for step in (1, 2):
+        res = drv.step()
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), fx[f"dry.step{step}.{k}"]) == 0, (step, k)
+    drv.close()
+
+
 def test_tall_columns_match_oracle():
     """130 levels (stride 136, 34 four-level chunks per column, more than a
     warp): the column sweeps run in their one-level form (k_vcoef,

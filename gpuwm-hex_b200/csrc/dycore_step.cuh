@@ -296,6 +296,16 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
     s_in = &so;
   }
 
+  // every output field but the scalars is final here (captured as an
+  // external event node, so that work outside the graph can wait on it)
+  if (ctx.dynamics_done && L.err == cudaSuccess) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    L.err = cudaStreamIsCapturing(L.st, &cap);
+    if (L.err == cudaSuccess)
+      L.err = cap == cudaStreamCaptureStatusActive
+                  ? cudaEventRecordWithFlags(ctx.dynamics_done, L.st, cudaEventRecordExternal)
+                  : cudaEventRecord(ctx.dynamics_done, L.st);
+  }
   // split scalar transport: RK1, RK2 standard, RK3 monotonic FCT
   if (nT > 0) {
     const float* q_prev = in.scalars;

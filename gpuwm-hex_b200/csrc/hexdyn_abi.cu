@@ -34,6 +34,9 @@ struct HexDynHandle {
   // private stream and events of hexdyn_step_batched
   cudaStream_t batch_stream = nullptr;
   cudaEvent_t batch_fork = nullptr, batch_done = nullptr;
+  // downloads of hexdyn_step_host that overlap the scalar transport
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_done = nullptr;
 };
 
 namespace {
@@ -542,6 +545,9 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
     HEX_CUDA(cudaStreamCreateWithFlags(&c.side_stream, cudaStreamNonBlocking), "side stream");
     for (auto& ev : c.fork_events) HEX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "fork event");
   }
+  HEX_CUDA(cudaEventCreateWithFlags(&c.dynamics_done, cudaEventDisableTiming), "dynamics event");
+  HEX_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+  HEX_CUDA(cudaEventCreateWithFlags(&h->copy_done, cudaEventDisableTiming), "copy event");
   HEX_CUDA(cudaDeviceSynchronize(), "create");
   return HEXDYN_OK;
 }
@@ -658,6 +664,32 @@ int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps) {
     h->ctx.parity ^= 1;
     h->ctx.steps_done++;
   }
+  return HEXDYN_OK;
+}
+
+int hexdyn_step_host(HexDynHandle* h, const float* const* in, float* const* out, void* stream) {
+  if (!h || !in || !out) return fail(HEXDYN_E_ARG, "NULL argument");
+  for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f)
+    if (h->staging_count[f] && (!in[f] || !out[f])) return fail(HEXDYN_E_ARG, "NULL host buffer of field %d", f);
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f)
+    if (h->staging_count[f] && (rc = hexdyn_set_state(h, f, in[f], h->staging_count[f], stream)) != HEXDYN_OK)
+      return rc;
+  if ((rc = hexdyn_step_async(h, stream, 1)) != HEXDYN_OK) return rc;
+  // every field but the scalars leaves on the copy stream once the step's
+  // dynamics end (beside the scalar transport); the scalars after the step
+  HEX_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ctx.dynamics_done, 0), "copy wait");
+  for (int f = 0; f < HEXDYN_NUM_FIELDS; ++f)
+    if (f != HEXDYN_SCALARS && h->staging_count[f] &&
+        (rc = hexdyn_get_state(h, f, out[f], h->staging_count[f], h->copy_stream)) != HEXDYN_OK)
+      return rc;
+  if (h->staging_count[HEXDYN_SCALARS] &&
+      (rc = hexdyn_get_state(h, HEXDYN_SCALARS, out[HEXDYN_SCALARS], h->staging_count[HEXDYN_SCALARS], stream)) !=
+          HEXDYN_OK)
+    return rc;
+  HEX_CUDA(cudaEventRecord(h->copy_done, h->copy_stream), "copy record");
+  HEX_CUDA(cudaStreamWaitEvent(st, h->copy_done, 0), "copy join");
   return HEXDYN_OK;
 }
 
@@ -905,6 +937,9 @@ int hexdyn_destroy(HexDynHandle* h) {
   for (auto& ev : c.fork_events)
     if (ev) cudaEventDestroy(ev);
   if (c.side_stream) cudaStreamDestroy(c.side_stream);
+  if (c.dynamics_done) cudaEventDestroy(c.dynamics_done);
+  if (h->copy_done) cudaEventDestroy(h->copy_done);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->host_flag) cudaFreeHost(h->host_flag);
   if (h->batch_fork) cudaEventDestroy(h->batch_fork);
   if (h->batch_done) cudaEventDestroy(h->batch_done);

@@ -95,6 +95,11 @@ struct HexCtx {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t fork_events[4] = {nullptr, nullptr, nullptr, nullptr};
   int concurrent_regions = 7;  // bit mask of the forked regions of a step
+  // Recorded on the step's stream once the last recovery of a step has
+  // written every output field but the scalars (an external event node of
+  // the step graph when captured); hexdyn_step_host starts the downloads of
+  // those fields on it while the scalar transport runs.
+  cudaEvent_t dynamics_done = nullptr;
   int threads_for(const char* label) const {
     if (force_threads) return force_threads;
     for (const auto& t : tuned_threads)

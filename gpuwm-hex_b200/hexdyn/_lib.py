@@ -22,6 +22,7 @@ FIELDS = {
     "theta_m": 5, "exner": 6, "density_perturbation": 7, "rho_theta_perturbation": 8,
     "pressure_perturbation": 9, "normal_velocity": 10, "vertical_velocity": 11,
 }
+HEXDYN_NUM_FIELDS = len(FIELDS)
 STATE_FIELDS = ("rho", "rho_theta", "rho_u", "rho_w", "scalars")
 SIDECAR_FIELDS = ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
                   "pressure_perturbation", "normal_velocity", "vertical_velocity")
@@ -82,6 +83,7 @@ EXPORTS = {
     "hexdyn_get_state": (C.c_int, [C.c_void_p, C.c_int, _F32P, C.c_size_t, C.c_void_p]),
     "hexdyn_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "hexdyn_step_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "hexdyn_step_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p]),
     "hexdyn_read_flag": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "hexdyn_capture_graph": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hexdyn_profile_steps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),

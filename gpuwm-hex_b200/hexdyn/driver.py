@@ -368,17 +368,24 @@ class HexDycoreDriver:
         """One large step from host buffers to host buffers, enqueued on the
         driver's stream without synchronising: upload of the state and sidecar,
         the step, download of both (the reference's from_host upload, step_device
-        and step() download, hexcore/cuda_driver.py:2826,5751,6112).  Use pinned
-        arrays for asynchronous copies; synchronise before reading the outputs."""
-        st = self._stream_handle()
-        for name, arr in (*state_in.items(), *side_in.items()):
-            _lib.check(self._lib.hexdyn_set_state(self._handle, _lib.FIELDS[name],
-                                                  arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, st))
-        _lib.check(self._lib.hexdyn_step_async(self._handle, st, 1))
+        and step() download, hexcore/cuda_driver.py:2826,5751,6112), through
+        ``hexdyn_step_host`` (the downloads of every field but the scalars
+        overlap the scalar transport).  Every field is given in and out; use
+        pinned arrays for asynchronous copies; synchronise before reading the
+        outputs."""
+        fin = (C.c_void_p * _lib.HEXDYN_NUM_FIELDS)()
+        fout = (C.c_void_p * _lib.HEXDYN_NUM_FIELDS)()
+        for src, dst in ((state_in, fin), (side_in, fin), (state_out, fout), (side_out, fout)):
+            for name, arr in src.items():
+                if arr.shape != self._shape(name) or arr.dtype != F32 or not arr.flags.c_contiguous:
+                    raise ValueError(f"{name}: expected a C-contiguous float32 array of shape {self._shape(name)}")
+                dst[_lib.FIELDS[name]] = arr.ctypes.data
+        names = (*_lib.STATE_FIELDS, *_lib.SIDECAR_FIELDS)
+        missing = [n for n in names if n not in {**state_in, **side_in} or n not in {**state_out, **side_out}]
+        if missing:
+            raise ValueError(f"step_host_buffers needs every field in and out; missing {missing}")
+        _lib.check(self._lib.hexdyn_step_host(self._handle, fin, fout, self._stream_handle()))
         self.time_seconds += self.config.config_dt
-        for name, arr in (*state_out.items(), *side_out.items()):
-            _lib.check(self._lib.hexdyn_get_state(self._handle, _lib.FIELDS[name],
-                                                  arr.ctypes.data_as(C.POINTER(C.c_float)), arr.size, st))
 
     def field_shape(self, name: str) -> tuple[int, ...]:
         return self._shape(name)

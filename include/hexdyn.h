@@ -177,6 +177,18 @@ int hexdyn_step(HexDynHandle* h, void* stream, int nsteps, int* flag_out, int* c
 /* Enqueue nsteps large steps without reading the flag (asynchronous). */
 int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps);
 
+/* One large step from host buffers to host buffers, enqueued on `stream`:
+ * the reference's from_host upload, step_device and step() download
+ * (hexcore/cuda_driver.py:2826, :5751, :6112) in one call.  `in` and `out`
+ * hold HEXDYN_NUM_FIELDS host pointers indexed by field identifier (logical
+ * layout as hexdyn_set_state / hexdyn_get_state; pinned memory for
+ * asynchronous copies; NULL allowed for an empty field).  Every field but
+ * the scalars is final when the step's dynamics end, so those downloads run
+ * on a private stream beside the scalar transport; the call returns with
+ * all of it ordered before later work on `stream` (synchronise `stream`
+ * before reading `out`). */
+int hexdyn_step_host(HexDynHandle* h, const float* const* in, float* const* out, void* stream);
+
 /* Read and clear the validation flag (synchronises `stream`). */
 int hexdyn_read_flag(HexDynHandle* h, void* stream, int* flag_out);
 

@@ -178,6 +178,47 @@ def test_graph_replay_is_bitwise_eager():
     graph.close()
 
 
+def _pinned(shape):
+    import torch
+
+    t = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    return t.numpy(), t
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_host_buffer_step_equals_device_step(graph):
+    """hexdyn_step_host (uploads, the step, and downloads of every field but
+    the scalars on a second stream beside the scalar transport) returns the
+    words of a device step followed by downloads, step after step, with the
+    outputs fed back as the next inputs."""
+    arr = case_arrays(build_case(build_mesh(4, lloyd=2, seed=0), n_levels=55, seed=0, n_condensates=2))
+    a = make_driver(arr, 1800.0, 2, "native", graph=graph)
+    b = make_driver(arr, 1800.0, 2, "native", graph=graph)
+    state, side = a.get_state()
+    hold, bufs = [], {}
+    for name in (*STATE, *SIDE):
+        src = getattr(state, name) if name in STATE else getattr(side, name)
+        x, t = _pinned(a.field_shape(name))
+        y, u = _pinned(a.field_shape(name))
+        x[...] = src
+        bufs[name] = (x, y)
+        hold += [t, u]
+    for step in (1, 2, 3):
+        a.step_host_buffers({k: bufs[k][0] for k in STATE}, {k: bufs[k][0] for k in SIDE},
+                            {k: bufs[k][1] for k in STATE}, {k: bufs[k][1] for k in SIDE})
+        a.synchronize()
+        res = b.step()
+        for k in STATE:
+            assert differing_words(bufs[k][1], getattr(res.state, k)) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(bufs[k][1], getattr(res.saved_diagnostics, k)) == 0, (step, k)
+        for k in (*STATE, *SIDE):
+            bufs[k][0][...] = bufs[k][1]
+            bufs[k][1][...] = np.nan
+    a.close()
+    b.close()
+
+
 def test_fast_numerics_within_tolerance(c1_case):
     strict = make_driver(c1_case, 1800.0, 2, "native")
     fast = make_driver(c1_case, 1800.0, 2, "native", numerics="fast")

@@ -971,6 +971,7 @@ struct MergedDesc {
   std::vector<float> dc, dv, area, area_tri, kite, weights, fv, fe, cosa, sina, adv, adv3;
   std::vector<float> zz, zxu, dss, zb, zb3, rb, rtb, eb;
   std::vector<float> smdiv_edge;
+  std::vector<float> deform_c2, deform_s2, deform_cs, mix_del2, mix_del4;
 };
 
 int check_compatible(const HexDynDesc& a, const HexDynDesc& b, int m) {
@@ -997,6 +998,17 @@ int check_compatible(const HexDynDesc& a, const HexDynDesc& b, int m) {
       !same_bits(a.rdzu, b.rdzu, L))
     return bad("the vertical coordinate");
   if (!same_bits(a.u_init, b.u_init, L) || !same_bits(a.v_init, b.v_init, L)) return bad("the reference winds");
+  if (b.horiz_mixing != a.horiz_mixing || b.rayleigh_levels != a.rayleigh_levels || b.cam_levels != a.cam_levels)
+    return bad("the mixing or upper-damping options");
+  const float ma[] = {a.rayleigh_inverse, a.horiz_mixing ? a.cam_base : 0.0f,
+                      a.horiz_mixing ? a.smag_strain_scale : 0.0f, a.horiz_mixing ? a.smag_ceiling : 0.0f,
+                      a.horiz_mixing ? a.smag_h4 : 0.0f, a.horiz_mixing ? a.smag_div_factor : 0.0f};
+  const float mb[] = {b.rayleigh_inverse, b.horiz_mixing ? b.cam_base : 0.0f,
+                      b.horiz_mixing ? b.smag_strain_scale : 0.0f, b.horiz_mixing ? b.smag_ceiling : 0.0f,
+                      b.horiz_mixing ? b.smag_h4 : 0.0f, b.horiz_mixing ? b.smag_div_factor : 0.0f};
+  // the Smagorinsky length scales with the mesh (config_len_disp or
+  // nominalMinDc), so a mixing ensemble holds meshes of one filter length
+  if (!same_bits(ma, mb, sizeof ma / sizeof ma[0])) return bad("the mixing or upper-damping constants");
   return HEXDYN_OK;
 }
 
@@ -1079,6 +1091,13 @@ int merge_members(const HexDynDesc* ds, int n, MergedDesc& M, HexDynHandle* h) {
   cat_slots_f(M.sina, ds, n, &HexDynDesc::sin_angle_edge, ne, w1, 1, E);
   cat_slots_f(M.adv, ds, n, &HexDynDesc::adv_coefs, ne, wA, mA, E);
   cat_slots_f(M.adv3, ds, n, &HexDynDesc::adv_coefs_3rd, ne, wA, mA, E);
+  if (a.horiz_mixing) {
+    cat_slots_f(M.deform_c2, ds, n, &HexDynDesc::deform_c2, nc, wE, mE, C);
+    cat_slots_f(M.deform_s2, ds, n, &HexDynDesc::deform_s2, nc, wE, mE, C);
+    cat_slots_f(M.deform_cs, ds, n, &HexDynDesc::deform_cs, nc, wE, mE, C);
+    cat_slots_f(M.mix_del2, ds, n, &HexDynDesc::mix_del2, ne, w1, 1, E);
+    cat_slots_f(M.mix_del4, ds, n, &HexDynDesc::mix_del4, ne, w1, 1, E);
+  }
   cat_rows(M.zz, ds, n, L, &HexDynDesc::zz, c0, nc, C);
   cat_rows(M.zxu, ds, n, L, &HexDynDesc::zxu, e0, ne, E);
   cat_rows(M.dss, ds, n, L, &HexDynDesc::dss, c0, nc, C);
@@ -1111,6 +1130,13 @@ int merge_members(const HexDynDesc* ds, int n, MergedDesc& M, HexDynHandle* h) {
   d.max_edges = mE;
   d.max_edges2 = mE2;
   d.adv_width = mA;
+  if (a.horiz_mixing) {
+    d.deform_c2 = M.deform_c2.data();
+    d.deform_s2 = M.deform_s2.data();
+    d.deform_cs = M.deform_cs.data();
+    d.mix_del2 = M.mix_del2.data();
+    d.mix_del4 = M.mix_del4.data();
+  }
   d.cells_on_edge = M.coe.data();
   d.edges_on_cell = M.eoc.data();
   d.cells_on_cell = M.coc.data();
@@ -1208,8 +1234,6 @@ int hexdyn_create_ensemble(const HexDynDesc* members, int n_members, HexDynHandl
   for (int m = 0; m < n_members; ++m) {
     int rc = validate(&members[m]);
     if (rc) return fail(rc, "ensemble member %d: %s", m, g_last_error.c_str());
-    if (members[m].horiz_mixing)
-      return fail(HEXDYN_E_ARG, "ensemble member %d: horizontal mixing is not merged across members", m);
     if (m > 0 && (rc = check_compatible(members[0], members[m], m))) return rc;
   }
   HexDynHandle* h = new HexDynHandle();
@@ -1568,6 +1592,14 @@ void carve(Carver& cv, const HexCtx& src, HexCtx& c) {
   w.edge_q = cv.take(T * ES);
   w.hres_lim = cv.take(T * ES);
   w.flag = (int*)cv.take(1);
+  if (g.smag_on) {
+    // 2-D Smagorinsky work arrays, one contiguous run (cleared per call)
+    struct { float** p; size_t n; } mix[] = {
+        {&w.vorticity, VS}, {&w.divergence, CS}, {&w.kdiff, CS}, {&w.delsq_u, ES}, {&w.delsq_div, CS},
+        {&w.delsq_vort, VS}, {&w.w_mix, CS}, {&w.delsq_w, CS}, {&w.theta_mix, CS}, {&w.delsq_theta, CS},
+        {&w.mix_u, ES}, {&w.mix_w, CS}};
+    for (auto& b : mix) *b.p = cv.take(b.n);
+  }
   for (int i = 0; i < 2; ++i) {
     HexState& t = c.tmp[i];
     t.rho = cv.take(CS);
@@ -1599,8 +1631,6 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
                                    int* flag_out) {
   if (!h || !in || !out) return fail(HEXDYN_E_ARG, "NULL handle or field set");
   const HexCtx& src = h->ctx;
-  if (src.geo.smag_on)
-    return fail(HEXDYN_E_ARG, "the no-allocation step does not carry the mixing work arrays; use hexdyn_step");
   HexState s_in, s_out;
   HexSide d_in, d_out;
   if (!fields_of(in, src.n_scalars, s_in, d_in) || !fields_of(out, src.n_scalars, s_out, d_out))
@@ -1642,6 +1672,11 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   const size_t CS = (size_t)g.nC * g.S, ES = (size_t)g.nE * g.S;
   // what must start at zero (or one): the flag and the dry coefficients
   HEX_CUDA(cudaMemsetAsync(c.w.flag, 0, sizeof(int), st), "clear flag");
+  if (g.smag_on) {
+    // the mixing arrays start cleared, as the allocating path's do
+    const size_t words = (size_t)(c.w.mix_w + CS - c.w.vorticity);
+    HEX_CUDA(cudaMemsetAsync(c.w.vorticity, 0, words * sizeof(float), st), "clear mixing");
+  }
   if (!g.moist) {
     HEX_CUDA(cudaMemsetAsync(c.w.qtot, 0, CS * sizeof(float), st), "clear qtot");
     k_fill<<<(unsigned)((CS + 255) / 256), 256, 0, st>>>(c.w.cqw, CS, 1.0f);

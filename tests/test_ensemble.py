@@ -66,6 +66,26 @@ def test_ensemble_members_equal_single_instances(cases):
     ens.close()
 
 
+def test_mixing_ensemble_members_equal_single_instances(cases):
+    """2-D Smagorinsky mixing in an ensemble: the deformation weights and
+    mesh scalings of each member are concatenated like its geometry, and
+    each member's words equal its own single-instance run."""
+    cfg = DycoreConfig(config_dt=900.0, config_number_of_sub_steps=2, moist_coefficients="native",
+                       config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=0.125,
+                       config_visc4_2dsmag=0.05)
+    members = [cases[0], cases[2]]  # one mesh: one Smagorinsky length
+    singles = [hexdyn.from_case(c, cfg) for c in members]
+    ens = HexEnsemble.from_cases(members, cfg, capture_graph=True)
+    ens.step_device(2)
+    for s in singles:
+        s.step_device(2)
+    for m in range(2):
+        _assert_same(ens, m, singles[m])
+    for s in singles:
+        s.close()
+    ens.close()
+
+
 def test_uneven_batch_equals_single_instances(cases):
     coarse, fine = _cfg(900.0), _cfg(450.0)
     g1 = HexEnsemble.from_cases([cases[0], cases[2]], coarse, capture_graph=True)

@@ -38,6 +38,30 @@ def test_ensemble_refuses_members_that_differ():
     assert not h.value
 
 
+def _mixing_desc(name, coef):
+    case = case_from_arrays(inputs(load_golden(name)))
+    cfg = DycoreConfig(config_dt=1800.0, config_number_of_sub_steps=2, config_horiz_mixing="2d_smagorinsky",
+                       config_smagorinsky_coef=coef, config_visc4_2dsmag=0.05)
+    return _build_descriptor(case.mesh, case, case.vertical, case, cfg, case, case, case)
+
+
+def test_mixing_ensemble_refuses_members_with_other_mixing():
+    """Members of a mixing ensemble share the option and its constants (the
+    Smagorinsky length scales with the mesh)."""
+    lib = L.load()
+    d0, k0, _ = _mixing_desc("l2_L12", 0.125)
+    d1, k1, _ = _desc("l2_L12", 1800.0)
+    h = C.c_void_p()
+    arr = (L.HexDynDesc * 2)(d0, d1)
+    assert lib.hexdyn_create_ensemble(arr, 2, C.byref(h)) == L.HEXDYN_E_ARG
+    assert "mixing or upper-damping options" in L.last_error()
+    d2, k2, _ = _mixing_desc("l2_L12", 0.1)
+    arr = (L.HexDynDesc * 2)(d0, d2)
+    assert lib.hexdyn_create_ensemble(arr, 2, C.byref(h)) == L.HEXDYN_E_ARG
+    assert "mixing or upper-damping constants" in L.last_error()
+    assert not h.value
+
+
 def test_batched_step_refuses_bad_batches():
     lib = L.load()
     assert lib.hexdyn_step_batched(None, None) == L.HEXDYN_E_ARG

@@ -24,8 +24,12 @@ from hexdyn.driver import DeviceAtmosphere
 pytestmark = pytest.mark.gpu
 
 
-def _driver(arr):
-    cfg = DycoreConfig(config_dt=1800.0, config_number_of_sub_steps=2, moist_coefficients="native")
+MIXING = dict(config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=0.125, config_visc4_2dsmag=0.05)
+
+
+def _driver(arr, mixing=False):
+    cfg = DycoreConfig(config_dt=1800.0, config_number_of_sub_steps=2, moist_coefficients="native",
+                       **(MIXING if mixing else {}))
     return hexdyn.from_case(case_from_arrays(arr), cfg)
 
 
@@ -37,15 +41,16 @@ def _logical(drv, name, padded):
     return padded[:, :rows].t().cpu().numpy()
 
 
-def test_noalloc_step_equals_step_on_two_calls():
+@pytest.mark.parametrize("mixing", [False, True])
+def test_noalloc_step_equals_step_on_two_calls(mixing):
     import torch
 
     if not torch.cuda.is_available():
         pytest.fail("this test needs a CUDA GPU")
     torch.cuda.set_device(0)
     arr = inputs(load_golden("l2_L12"))
-    ref = _driver(arr)
-    noa = _driver(arr)
+    ref = _driver(arr, mixing)
+    noa = _driver(arr, mixing)
     atm = DeviceAtmosphere(noa)
     names = list(L.FIELDS)
     # caller-owned buffers in the padded layout, the input filled from the

@@ -86,6 +86,7 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_diag_edge": 3 * el + vl + cl + conn_e,                  # u, cached v, pv_edge out
         "k_diag_edge_v": 3 * el + vl + cl + conn_e + E * 24,       # u (+ neighbours), v out, pv_edge out
         "k_moist_cell": tcl + 2 * cl,
+        "k_clamp_scalars": 2 * tcl,
         "k_moist_edge": tcl + el + conn_e,
         "k_euler_edge": 3 * el + 4 * cl + conn_e,
         "k_euler_cell": el + 2 * ci + 5 * cl + conn_c,

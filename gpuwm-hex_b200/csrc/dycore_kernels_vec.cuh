@@ -112,6 +112,19 @@ __device__ __forceinline__ Win win(const float* __restrict__ col, int k0, int S)
   return w;
 }
 
+// End-of-step clamp of negative mixing ratios (hexcore/cuda_driver.py:5311,
+// `putmask(scalars, scalars < 0, 0)`): -0 and NaN compare false and stay.
+// blockIdx.z selects the scalar.
+__global__ void HEX_VEC_BOUNDS kv_clamp_scalars(HexGeo g, float* __restrict__ q) {
+  HEX_VEC_PARALLEL(g.nC)
+  float* p = q + ((size_t)blockIdx.z * g.nC + ent) * g.S + k0;
+  V4 v = ld4rw(p);
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (v.a[j] < 0.0f) v.a[j] = 0.0f;
+  st4m(p, v, k0, 0, g.L);
+}
+
 // --------------------------------------------------- moist coefficients
 // hexcore/regional_v841.py:1180 compute_moist_coefficients, every scalar:
 // qtot = sum of the scalars in scalar order, cqw = 1/(1 + (qtot(k) +

@@ -336,6 +336,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       }
       q_prev = q_next;
     }
+    if (g.clamp_scalars) L.lpv("k_clamp_scalars", g.nC, nT, kv_clamp_scalars, g, out.scalars);
   }
   if (launches) *launches = L.count;
   return L.err;

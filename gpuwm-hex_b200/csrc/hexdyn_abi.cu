@@ -260,6 +260,8 @@ int validate(const HexDynDesc* d) {
                 d->cam_levels);
   if (d->cam_levels && !d->horiz_mixing)
     return fail(HEXDYN_E_ARG, "the CAM floor applies to the Smagorinsky diffusivity: mixing must be on");
+  if (d->clamp_negative_scalars != 0 && d->clamp_negative_scalars != 1)
+    return fail(HEXDYN_E_ARG, "clamp_negative_scalars=%d must be 0 or 1", d->clamp_negative_scalars);
   if (d->horiz_mixing != 0 && d->horiz_mixing != 1)
     return fail(HEXDYN_E_ARG, "horiz_mixing=%d must be 0 (off) or 1 (2-D Smagorinsky)", d->horiz_mixing);
   if (d->horiz_mixing) {
@@ -469,6 +471,7 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
     g.smag_h4 = d.smag_h4;
     g.smag_div_factor = d.smag_div_factor;
   }
+  g.clamp_scalars = d.clamp_negative_scalars;
   g.rayleigh_levels = d.rayleigh_levels;
   g.rayleigh_inverse = d.rayleigh_inverse;
   g.cam_levels = d.cam_levels;
@@ -986,7 +989,9 @@ int check_compatible(const HexDynDesc& a, const HexDynDesc& b, int m) {
   if (b.n_sub_steps != a.n_sub_steps || b.split_steps != a.split_steps ||
       (b.time_integration_order == 2) != (a.time_integration_order == 2))
     return bad("the schedule");
-  if (b.monotonic != a.monotonic || b.moist != a.moist || b.numerics != a.numerics) return bad("the options");
+  if (b.monotonic != a.monotonic || b.moist != a.moist || b.numerics != a.numerics ||
+      b.clamp_negative_scalars != a.clamp_negative_scalars)
+    return bad("the options");
   const float fa[] = {a.coef_3rd_order, a.apvm_upwinding, a.smdiv, a.len_disp, a.epssm_minimum, a.epssm_maximum,
                       a.epssm_bottom_z, a.epssm_top_z, a.rgas, a.cp, a.gravity, a.p0, a.cf1, a.cf2, a.cf3,
                       a.acoustic_dts2[0], a.acoustic_dts2[1], a.acoustic_dts2[2]};

@@ -10,7 +10,7 @@ from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libhexdyn.so"
 
-HEXDYN_ABI_VERSION = 4
+HEXDYN_ABI_VERSION = 5
 HEXDYN_OK = 0
 HEXDYN_E_ARG = -1
 HEXDYN_E_STATE = -2
@@ -64,7 +64,7 @@ class HexDynDesc(C.Structure):
         ("mix_del2", _F32P), ("mix_del4", _F32P), ("smag_strain_scale", C.c_float), ("smag_ceiling", C.c_float),
         ("smag_h4", C.c_float), ("smag_div_factor", C.c_float),
         ("rayleigh_levels", C.c_int32), ("rayleigh_inverse", C.c_float), ("cam_levels", C.c_int32),
-        ("cam_base", C.c_float),
+        ("cam_base", C.c_float), ("clamp_negative_scalars", C.c_int32),
     ]
 
 

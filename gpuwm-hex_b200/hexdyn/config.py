@@ -68,6 +68,13 @@ class DycoreConfig:
     config_number_rayleigh_damp_u_levels: int = 6
     config_rayleigh_damp_u_timescale_days: float = 5.0
     config_moist_physics: bool = False
+    # End-of-step clamp of negative mixing ratios (where q < 0: q = 0) that
+    # the reference's CUDA driver applies on the global path without physics
+    # (hexcore/cuda_driver.py:5306-5311); its NumPy authority, which the
+    # strict parity follows, applies it only with config_moist_physics
+    # (hexcore/driver.py:3531-3534).  The monotonic limiter's output is never
+    # negative, so the clamp changes words only with standard transport.
+    clamp_negative_scalars: bool = False
     config_rayleigh_damp_u: bool = False
     config_apply_lbcs: bool = False
     # Coefficient semantics of the carried scalars: "native" applies

@@ -533,5 +533,6 @@ def _build_descriptor(mesh, state, vertical, reference, cfg: DycoreConfig, terra
         days = F32(cfg.config_rayleigh_damp_u_timescale_days)
         desc.rayleigh_levels = levels
         desc.rayleigh_inverse = float(F32(1.0) / (F32(levels) * (days * F32(86400.0))))
+    desc.clamp_negative_scalars = 1 if cfg.clamp_negative_scalars else 0
     sizes = dict(n_cells=ncells, n_edges=nedges, n_vertices=nvert, n_levels=nlev, n_scalars=int(scalars.shape[0]))
     return desc, keep, sizes

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define HEXDYN_ABI_VERSION 4
+#define HEXDYN_ABI_VERSION 5
 
 #define HEXDYN_OK 0
 #define HEXDYN_E_ARG (-1)        /* invalid argument or descriptor */
@@ -145,6 +145,12 @@ typedef struct HexDynDesc {
   float rayleigh_inverse;
   int32_t cam_levels;
   float cam_base;
+  /* 1: set negative mixing ratios to zero at the end of the step (where
+   * q < 0: q = 0; -0 and NaN kept), as the reference's CUDA driver does on
+   * the global path without physics (hexcore/cuda_driver.py:5306-5311,
+   * atm_srk3 2798-2800); its NumPy authority does so only with
+   * config_moist_physics (hexcore/driver.py:3531-3534).  0: no clamp. */
+  int32_t clamp_negative_scalars;
 } HexDynDesc;
 
 typedef struct HexDynHandle HexDynHandle;

@@ -75,6 +75,7 @@ class OracleConfig:
     order: int = 3              # config_time_integration_order (2 or 3)
     smagorinsky: Any = None     # oracle.mixing.SmagorinskyConfig: 2-D Smagorinsky mixing on
     rayleigh: Any = None        # (levels, days): Rayleigh damping of u over the top levels
+    clamp_negative_scalars: bool = False  # cuda_driver.py:5311 end-of-step clamp
 
 
 def schedule(dt: float, n_sub: int, splits: int, order: int = 3):
@@ -913,6 +914,11 @@ class OracleDycore:
                     q = self.advance_scalars_mono(outer.scalars, q, outer.rho, cur.rho, flux_u, flux_w, large_dt)
                 else:
                     q = self.advance_scalars(outer.scalars, q, outer.rho, cur.rho, flux_u, flux_w, large_dt, stage)
+            if cfg.clamp_negative_scalars:
+                # hexcore/cuda_driver.py:5311 putmask(scalars, scalars < 0, 0):
+                # -0 and NaN compare false and keep their words
+                q = q.copy()
+                q[q < 0] = ZERO
             cur.scalars = q
         if record is not None:
             record.append(dict(flux_u=flux_u, flux_w=flux_w))

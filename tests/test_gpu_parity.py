@@ -123,6 +123,32 @@ def test_cells_on_cell_slot_order_does_not_change_the_step():
     drv.close()
 
 
+def test_negative_scalar_clamp_matches_oracle():
+    """clamp_negative_scalars (the reference CUDA driver's end-of-step
+    `putmask(scalars, scalars < 0, 0)`) with standard transport, whose
+    undershoots leave negative mixing ratios: the CUDA step equals the
+    oracle with the clamp, and the oracle without it holds negatives (so the
+    clamp is exercised)."""
+    arr = case_arrays(build_case(build_mesh(2, lloyd=2, seed=0), n_levels=12, seed=0, n_condensates=2))
+    knobs = dict(dt=1800.0, n_sub_steps=2, moist="native", monotonic=False)
+    raw, _ = OracleDycore(arr, OracleConfig(**knobs)).step(State(*(np.asarray(arr[k]).copy() for k in STATE)))
+    assert (raw.scalars < 0).sum() > 0
+    orc = OracleDycore(arr, OracleConfig(**knobs, clamp_negative_scalars=True))
+    cfg = DycoreConfig(config_dt=1800.0, config_number_of_sub_steps=2, moist_coefficients="native",
+                       config_monotonic=False, clamp_negative_scalars=True)
+    drv = hexdyn.from_case(case_from_arrays(arr), cfg, capture_graph=True)
+    st, sd = State(*(np.asarray(arr[k]).copy() for k in STATE)), None
+    for step in (1, 2):
+        st, sd = orc.step(st, sd)
+        assert (st.scalars < 0).sum() == 0
+        res = drv.step()
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), getattr(st, k)) == 0, (step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), getattr(sd, k)) == 0, (step, k)
+    drv.close()
+
+
 def test_tall_columns_match_oracle():
     """130 levels (stride 136, 34 four-level chunks per column, more than a
     warp): the column sweeps run in their one-level form (k_vcoef,

@@ -107,3 +107,24 @@ def test_smagorinsky_steps_match_reference():
             assert differing_words(getattr(state, k), fx[f"dry.step{step}.{k}"]) == 0, (step, k)
         for k in SIDE:
             assert differing_words(getattr(side, k), fx[f"dry.step{step}.side.{k}"]) == 0, (step, k)
+
+
+def test_oracle_scalar_clamp_zeroes_only_negatives():
+    """The end-of-step clamp (`putmask(scalars, scalars < 0, 0)`,
+    hexcore/cuda_driver.py:5311) is the step's last operation: the clamped
+    step equals the unclamped one with exactly its negative words zeroed."""
+    from hexdyn.case import build_case, case_arrays
+    from hexdyn.mesh import build_mesh
+
+    arr = case_arrays(build_case(build_mesh(2, lloyd=2, seed=0), n_levels=12, seed=0, n_condensates=2))
+    knobs = dict(dt=1800.0, n_sub_steps=2, moist="native", monotonic=False)
+    start = State(*(np.asarray(arr[k]).copy() for k in STATE))
+    raw, raw_side = OracleDycore(arr, OracleConfig(**knobs)).step(start.copy())
+    clamped, side = OracleDycore(arr, OracleConfig(**knobs, clamp_negative_scalars=True)).step(start.copy())
+    neg = raw.scalars < 0
+    assert neg.sum() > 0
+    expect = np.where(neg, np.float32(0.0), raw.scalars)
+    assert differing_words(clamped.scalars, expect) == 0
+    for k in STATE:
+        if k != "scalars":
+            assert differing_words(getattr(clamped, k), getattr(raw, k)) == 0, k

@@ -149,6 +149,25 @@ def test_negative_scalar_clamp_matches_oracle():
     drv.close()
 
 
+@pytest.mark.parametrize("levels", [4, 5, 8])
+def test_short_columns_match_oracle(levels):
+    """The fewest levels the third-order vertical fluxes allow (4), and 5 and
+    8: one or two four-level chunks per column, every chunk holding a
+    boundary interface."""
+    arr = case_arrays(build_case(build_mesh(2, lloyd=2, seed=0), n_levels=levels, seed=0, n_condensates=1))
+    drv = make_driver(arr, 900.0, 2, "native", graph=True)
+    orc = OracleDycore(arr, OracleConfig(dt=900.0, n_sub_steps=2, moist="native"))
+    state, side = State(*(np.asarray(arr[k]).copy() for k in STATE)), None
+    for step in (1, 2):
+        res = drv.step()
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(res.state, k), getattr(state, k)) == 0, (levels, step, k)
+        for k in SIDE:
+            assert differing_words(getattr(res.saved_diagnostics, k), getattr(side, k)) == 0, (levels, step, k)
+    drv.close()
+
+
 def test_tall_columns_match_oracle():
     """130 levels (stride 136, 34 four-level chunks per column, more than a
     warp): the column sweeps run in their one-level form (k_vcoef,

@@ -313,24 +313,54 @@ class HexDycoreDriver:
                           acoustic_output_callback: Any = None) -> DeviceStepResult:
         """One large step with the reference's production signature
         (hexcore/cuda_driver.py:4854, called by
-        hexcore/mpasphys/runtime_v842.py:2310).  The physics hand-offs are
-        outside this path and refused by name before any launch;
-        ``acoustic_output_callback(ru_p=..., rw_p=...)`` receives the final
-        acoustic words after the step (the reference calls it after RK stage
-        3 of every dynamics subcycle; its last call carries these values)."""
+        hexcore/mpasphys/runtime_v842.py:2310).  Held physics tendencies and
+        the per-stage physics callback are outside this path and refused by
+        name before any launch.  ``physics_post_transport_callback(state=,
+        saved=, outer_state=, modified_theta_dynamics_rate=)`` is called after
+        the scalar transport, as the reference does (cuda_driver.py:5299-5305):
+        ``state`` and ``saved`` hold logical [level][entity] device views of
+        the step's result (writes land in the library's buffers and feed the
+        next step), ``outer_state`` views of the state the step started from,
+        and ``modified_theta_dynamics_rate`` is None (the reference forms it
+        only with physics tendencies).  ``acoustic_output_callback(ru_p=...,
+        rw_p=...)`` receives the final acoustic words after the step (the
+        reference calls it after RK stage 3 of every dynamics subcycle; its
+        last call carries these values)."""
+        from .config import ConfigurationRefusal
+
         for knob, value in (("physics_tendencies", physics_tendencies),
                             ("physics_stage_callback", physics_stage_callback),
-                            ("physics_post_transport_callback", physics_post_transport_callback),
                             ("physics_mass_loading_count", physics_mass_loading_count)):
             if value is not None:
-                from .config import ConfigurationRefusal
-
                 raise ConfigurationRefusal(knob, value, "the physics coupling is not on the dry dycore step path",
                                            f"{knob}=None")
+        outer = None
+        if physics_post_transport_callback is not None:
+            if self.config.clamp_negative_scalars:
+                # the reference skips its end-of-step clamp when the callback
+                # takes the transported scalars (cuda_driver.py:5306-5311)
+                raise ConfigurationRefusal("clamp_negative_scalars", True, "a post-transport callback receives "
+                                           "the unclamped scalars", "clamp_negative_scalars=False")
+            outer = self._views(_lib.STATE_FIELDS)  # the step reads these buffers and writes the others
         res = self.step_device(1)
+        if physics_post_transport_callback is not None:
+            physics_post_transport_callback(state=self._views(_lib.STATE_FIELDS),
+                                            saved=self._views(_lib.SIDECAR_FIELDS), outer_state=outer,
+                                            modified_theta_dynamics_rate=None)
         if acoustic_output_callback is not None:
             acoustic_output_callback(**self.acoustic_words())
         return res
+
+    def _views(self, names) -> Any:
+        """Logical device views of the current buffers of ``names`` (with
+        ``time_seconds`` for the state)."""
+        from types import SimpleNamespace
+
+        atm = DeviceAtmosphere(self)
+        fields = {n: atm.logical(n) for n in names if not (n == "scalars" and self.sizes["n_scalars"] == 0)}
+        if "rho" in names:
+            fields["time_seconds"] = self.time_seconds
+        return SimpleNamespace(**fields)
 
     def profile(self, nsteps: int = 1) -> dict[str, tuple[int, float]]:
         """Per-kernel launches and total milliseconds over ``nsteps`` eager

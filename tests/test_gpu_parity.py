@@ -292,6 +292,41 @@ def test_runs_are_deterministic(c1_case):
         assert differing_words(getattr(outs[0].state, k), getattr(outs[1].state, k)) == 0
 
 
+def test_post_transport_callback_sees_the_step_and_writes_through():
+    """physics_post_transport_callback receives logical device views of the
+    step's result and of the state the step started from (the reference's
+    hand-off after transport); writes into the result land in the library's
+    buffers."""
+    from hexdyn.config import ConfigurationRefusal
+
+    fx = load_golden("l2_L12")
+    drv = make_driver(inputs(fx), float(fx["config.dt"]), int(fx["config.n_sub_steps"]), "dry", graph=True)
+    before, _ = drv.get_state()
+    seen = {}
+
+    def hand_off(state, saved, outer_state, modified_theta_dynamics_rate):
+        seen["rho"] = state.rho.cpu().numpy()
+        seen["outer_rho"] = outer_state.rho.cpu().numpy()
+        seen["outer_scalars"] = outer_state.scalars.cpu().numpy()
+        seen["u"] = saved.normal_velocity.cpu().numpy()
+        seen["rate"] = modified_theta_dynamics_rate
+        state.scalars.zero_()
+
+    drv._step_device_v841(physics_post_transport_callback=hand_off)
+    after, _ = drv.get_state()
+    assert differing_words(seen["outer_rho"], before.rho) == 0
+    assert differing_words(seen["outer_scalars"], before.scalars) == 0
+    assert differing_words(seen["rho"], fx["dry.step1.rho"]) == 0
+    assert differing_words(seen["u"], fx["dry.step1.side.normal_velocity"]) == 0
+    assert seen["rate"] is None
+    assert after.scalars.size > 0 and not after.scalars.any()
+    drv.close()
+    clamp = hexdyn.from_case(case_from_arrays(inputs(fx)), DycoreConfig(config_dt=1800.0, clamp_negative_scalars=True))
+    with pytest.raises(ConfigurationRefusal):
+        clamp._step_device_v841(physics_post_transport_callback=hand_off)
+    clamp.close()
+
+
 def test_validation_flag_raises_on_bad_state():
     """A host-side corruption (negative rho_theta in one column) must come back
     as the device validation flag, not as a silent result or a fault."""
@@ -306,7 +341,7 @@ def test_validation_flag_raises_on_bad_state():
 
 def test_acoustic_words_and_reference_step_signature():
     """_step_device_v841 (the reference's production entry) refuses the
-    physics hand-offs by name and hands acoustic_output_callback the final
+    held-tendency physics hand-offs by name and hands acoustic_output_callback the final
     acoustic words, equal to the oracle's ru_p and rw_p after the last
     substep of RK stage 3 of the last subcycle."""
     from hexdyn.config import ConfigurationRefusal
@@ -315,7 +350,7 @@ def test_acoustic_words_and_reference_step_signature():
     fx = load_golden("l2_L12")
     arr = inputs(fx)
     drv = make_driver(arr, float(fx["config.dt"]), int(fx["config.n_sub_steps"]), "dry", graph=True)
-    for kw in ("physics_stage_callback", "physics_post_transport_callback", "physics_mass_loading_count"):
+    for kw in ("physics_stage_callback", "physics_mass_loading_count"):
         with pytest.raises(ConfigurationRefusal) as err:
             drv._step_device_v841(**{kw: 1})
         assert err.value.knob == kw

@@ -45,6 +45,8 @@ def test_calls_on_null_handle_are_refused():
     x = np.zeros(4, dtype=np.float32)
     assert lib.hexdyn_set_state(None, 0, x.ctypes.data_as(C.POINTER(C.c_float)), 4, None) == L.HEXDYN_E_ARG
     assert lib.hexdyn_step(None, None, 1, None, None) == L.HEXDYN_E_ARG
+    ptrs = (C.c_void_p * L.HEXDYN_NUM_FIELDS)()
+    assert lib.hexdyn_step_host(None, ptrs, ptrs, None) == L.HEXDYN_E_ARG
     assert lib.hexdyn_destroy(None) == L.HEXDYN_OK
 
 

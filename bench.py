@@ -106,9 +106,9 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_tr_edge_mono": (tcl + tel) + el + adv,
         "k_tr_std": 3 * tcl + tel + 2 * cl + el + ci + conn_c,
         "k_fct_target": 2 * cl + el + ci + conn_c,
-        "k_fct_cell1": 5 * tcl + tel + 2 * cl + el + ci + conn_c,
+        "k_fct_cell1": 5 * tcl + T * ci + tel + 2 * cl + el + ci + conn_c,   # + vertical fluxes out
         "k_fct_edge": 3 * tcl + 2 * tel + el + conn_e,
-        "k_fct_cell2": 6 * tcl + tel + cl + ci + conn_c,
+        "k_fct_cell2": 4 * tcl + T * ci + tel + cl + conn_c,             # vertical fluxes in
         # 2-D Smagorinsky mixing (bench --smagorinsky), once per subcycle
         "k_smag_kdiff": 2 * el + cl + 3 * C * maxE + conn_c,
         "k_mix_edge2": 3 * cl + vl + 3 * el + conn_e + E * 2,

@@ -1300,7 +1300,8 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
                              const float* __restrict__ q_stage, const float* __restrict__ rho_old,
                              const float* __restrict__ hv, const float* __restrict__ ww,
                              const float* __restrict__ high_e, const float* __restrict__ target,
-                             float* __restrict__ scale_in, float* __restrict__ scale_out, float* __restrict__ mass_out) {
+                             float* __restrict__ scale_in, float* __restrict__ scale_out, float* __restrict__ mass_out,
+                             float* __restrict__ vres_out) {
   HEX_VEC_TRACER(g.nC, nT)
   const int c = ent, S = g.S, L = g.L;
   const int ii = c * S + k0;
@@ -1334,6 +1335,9 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell1(HexGeo g, int nT, float step, const 
   float mass[4], s_in[4], s_out[4], vr[5];
 #pragma unroll
   for (int d = 0; d < 5; ++d) vr[d] = fct_vres_win(g, step, qw, ow, www, k0, d);
+  // interfaces k0..k0+3 for the limited update (every interface of the
+  // column is some thread's k0 + d, d < 4)
+  st4(vres_out + toff + ii, V4{{vr[0], vr[1], vr[2], vr[3]}});
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int k = k0 + j;
@@ -1416,8 +1420,8 @@ __global__ void __launch_bounds__(256, HEX_FCT_EDGE_MIN_BLOCKS) kv_fct_edge(HexG
 }
 
 // hexcore/transport.py:1919-2118: limited update of the monotonic stage.
-__global__ void HEX_VEC_BOUNDS kv_fct_cell2(HexGeo g, int nT, float step, const float* __restrict__ q_old,
-                             const float* __restrict__ q_stage, const float* __restrict__ ww,
+// The vertical residual fluxes are those kv_fct_cell1 formed (vres).
+__global__ void HEX_VEC_BOUNDS kv_fct_cell2(HexGeo g, int nT, const float* __restrict__ vres,
                              const float* __restrict__ scale_in, const float* __restrict__ scale_out,
                              const float* __restrict__ mass_in, const float* __restrict__ hres_lim,
                              const float* __restrict__ target, float* __restrict__ q_out) {
@@ -1437,13 +1441,16 @@ __global__ void HEX_VEC_BOUNDS kv_fct_cell2(HexGeo g, int nT, float step, const 
 #pragma unroll
     for (int j = 0; j < 4; ++j) mass.a[j] = mass.a[j] + ts * h.a[j] * ia;
   }
-  const Win ow = win(q_old + toff + c * S, k0, S), qw = win(q_stage + toff + c * S, k0, S);
-  const Win www = win(ww + c * S, k0, S);
   const Win siw = win(scale_in + toff + c * S, k0, S), sow = win(scale_out + toff + c * S, k0, S);
+  // interface k0 + 4 belongs to the next chunk; past the column's last chunk
+  // it only feeds a padding level, never stored
+  const float* vc = vres + toff + c * S;
+  const V4 f4 = ld4(vc + k0);
+  const float fv[5] = {f4.a[0], f4.a[1], f4.a[2], f4.a[3], k0 + 4 < S ? vc[k0 + 4] : 0.0f};
   float vl[5];
 #pragma unroll
   for (int d = 0; d < 5; ++d) {
-    const float f = fct_vres_win(g, step, qw, ow, www, k0, d);
+    const float f = fv[d];
     const int j = k0 + d;
     vl[d] = (j <= 0 || j >= g.L) ? f
                                  : pos0(f) * pymin(sow(d - 1), siw(d)) + neg0(f) * pymin(sow(d), siw(d - 1));

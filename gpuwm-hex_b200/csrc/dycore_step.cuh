@@ -327,11 +327,10 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
                (const float*)w.flux_u, w.edge_q);
         L.lpvt("k_fct_cell1", g.nC, nT, g.coc_across ? kv_fct_cell1<true> : kv_fct_cell1<false>, g, nT, step,
              (const float*)in.scalars, q_prev, (const float*)in.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
-             w.scale_in, w.scale_out, w.mass);
+             w.scale_in, w.scale_out, w.mass, w.vres);
         LPST(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
-        LPST(L, g.nC, nT, fct_cell2, g, step, (const float*)in.scalars, q_prev, (const float*)w.flux_w,
-             (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
+        LPST(L, g.nC, nT, fct_cell2, g, (const float*)w.vres, (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,
              (const float*)w.target, q_next);
       }
       q_prev = q_next;

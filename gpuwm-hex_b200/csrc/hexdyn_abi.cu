@@ -517,7 +517,7 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
       {&w.gamma_tri, CS}, {&w.ru_p, ES}, {&w.ru_avg, ES}, {&w.rw_p, CS}, {&w.ww_avg, CS}, {&w.rho_pp, CS},
       {&w.rtpp[0], CS}, {&w.rtpp[1], CS}, {&w.flux_u, ES}, {&w.flux_w, CS}, {&w.q_stage[0], T * CS},
       {&w.q_stage[1], T * CS}, {&w.edge_q, T * ES}, {&w.target, CS}, {&w.scale_in, T * CS},
-      {&w.scale_out, T * CS}, {&w.mass, T * CS}, {&w.hres_lim, T * ES}};
+      {&w.scale_out, T * CS}, {&w.mass, T * CS}, {&w.hres_lim, T * ES}, {&w.vres, T * CS}};
   for (auto& b : bufs)
     if ((e = dev_alloc(c, b.p, b.n))) return cuda_fail(e, "alloc work");
   if ((e = dev_alloc(c, &w.flag, 1))) return cuda_fail(e, "alloc flag");
@@ -1592,7 +1592,7 @@ void carve(Carver& cv, const HexCtx& src, HexCtx& c) {
   for (float** p : edge) *p = cv.take(ES);
   w.pv_vertex = cv.take(VS);
   w.ke_vertex = cv.take(VS);
-  float** tcell[] = {&w.q_stage[0], &w.q_stage[1], &w.scale_in, &w.scale_out, &w.mass};
+  float** tcell[] = {&w.q_stage[0], &w.q_stage[1], &w.scale_in, &w.scale_out, &w.mass, &w.vres};
   for (float** p : tcell) *p = cv.take(T * CS);
   w.edge_q = cv.take(T * ES);
   w.hres_lim = cv.take(T * ES);

@@ -43,6 +43,7 @@ struct HexWork {
   float *flux_u, *flux_w;
   // transport
   float *q_stage[2], *edge_q, *target, *scale_in, *scale_out, *mass, *hres_lim;
+  float* vres;  // [T][C][S] the limiter's vertical residual flux at interfaces 0..S-1
   int* flag;            // device validation flag (bit set, see HEX_FLAG_*)
   // 2-D Smagorinsky mixing (allocated when on): diagnostics of the
   // subcycle's start, diffusivity, Laplacians and the saved mixed terms

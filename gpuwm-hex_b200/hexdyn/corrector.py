@@ -148,6 +148,27 @@ def make_pairs(full: HexDycoreDriver, reduced: HexDycoreDriver, states, *, sampl
     return out
 
 
+def rank_batches(n_batches: int, rank: int, world: int) -> list[int]:
+    """Data-parallel shard of an epoch's batches: rank r takes batches
+    r, r + W, ... and every rank takes the same count (the remainder is
+    dropped), so all ranks join the same number of gradient reductions."""
+    per_rank = n_batches // world
+    return [rank + i * world for i in range(per_rank)]
+
+
+def average_gradients(tensors, group=None) -> None:
+    """Sum every tensor over the ranks of ``group`` and divide by the rank
+    count, in place (one all-reduce per tensor, in list order on every rank).
+    Each rank's gradient is the mean over its own batch, so the average is
+    the mean over the global batch."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    for t in tensors:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        t.div_(world)
+
+
 def _stats(x: np.ndarray, floor: float = 1e-12):
     mean = x.mean(axis=0).astype(np.float32)
     std = x.std(axis=0).astype(np.float32)
@@ -173,8 +194,19 @@ class TrainedNet:
         self.n_in, self.n_out = n_in, n_out
 
     def fit(self, x: np.ndarray, y: np.ndarray, *, epochs: int, batch: int, lr: float, val_frac: float = 0.2,
-            seed: int = 0) -> NetTraining:
+            seed: int = 0, group=None) -> NetTraining:
+        """Adam on the mean squared error of normalised targets.  With a
+        process group of W > 1 ranks (every rank given the same pairs and
+        seed, hence the same split and initial weights) each rank runs its
+        shard of every epoch's batches and the weight and bias gradients are
+        averaged over the ranks before each optimizer step, so the weights
+        stay identical on every rank (data parallel)."""
         import torch
+        import torch.distributed as dist
+
+        world, rank = 1, 0
+        if group is not None or (dist.is_available() and dist.is_initialized()):
+            world, rank = dist.get_world_size(group), dist.get_rank(group)
 
         rng = np.random.default_rng(seed)
         perm = rng.permutation(len(x))
@@ -224,13 +256,16 @@ class TrainedNet:
         rec.val_loss_initial = val_loss()
         rec.val_loss_zero = float(np.mean((y[val] / self.y_scale) ** 2))
         t0 = time.perf_counter()
+        grads = [t for lay in net.layers for t in (lay.gw, lay.gb)]
         for ep in range(epochs):
             order = rng.permutation(tr)
             ep_loss, ep_n = 0.0, 0
-            for s in range(0, len(order) - B + 1, B):
-                idx = order[s:s + B]
+            for b in rank_batches(len(order) // B, rank, world):
+                idx = order[b * B:(b + 1) * B]
                 n = load_batch(idx)
                 loss = net.gradients(Xb, Xt, Tb, n)
+                if world > 1:
+                    average_gradients(grads, group)
                 net.adam(lr * 0.5 * (1.0 + np.cos(np.pi * ep / epochs)))
                 rec.steps += 1
                 ep_loss += float(loss.item())

@@ -195,17 +195,19 @@ class TrainedNet:
 
     def fit(self, x: np.ndarray, y: np.ndarray, *, epochs: int, batch: int, lr: float, val_frac: float = 0.2,
             seed: int = 0, group=None) -> NetTraining:
-        """Adam on the mean squared error of normalised targets.  With a
-        process group of W > 1 ranks (every rank given the same pairs and
-        seed, hence the same split and initial weights) each rank runs its
-        shard of every epoch's batches and the weight and bias gradients are
-        averaged over the ranks before each optimizer step, so the weights
-        stay identical on every rank (data parallel)."""
+        """Adam on the mean squared error of normalised targets.  Given a
+        process group of W > 1 ranks (``group=torch.distributed.group.WORLD``
+        for all of them; every rank given the same pairs and seed, hence the
+        same split and initial weights) each rank runs its shard of every
+        epoch's batches and the weight and bias gradients are averaged over
+        the ranks before each optimizer step, so the weights stay identical
+        on every rank (data parallel).  Without a group the rank trains
+        alone."""
         import torch
         import torch.distributed as dist
 
         world, rank = 1, 0
-        if group is not None or (dist.is_available() and dist.is_initialized()):
+        if group is not None:
             world, rank = dist.get_world_size(group), dist.get_rank(group)
 
         rng = np.random.default_rng(seed)

@@ -65,3 +65,25 @@ def test_rk2_schedule_matches_mpas(dt, substeps):
     assert [np.float32(s[1]).tobytes() for s in st] == [w.tobytes() for w in want]
     assert np.float32(schedule(dt, substeps, 1, order=2)[0][1]) == np.float32(dt * 0.5)
     DycoreConfig(config_dt=dt, config_time_integration_order=2, config_number_of_sub_steps=substeps).validate()
+
+
+def test_bench_byte_model_covers_every_step_kernel():
+    """bench.py's roofline needs the algorithmic bytes of every launch label
+    the step can issue (the labels of csrc/dycore_step.cuh)."""
+    import re
+    from pathlib import Path
+
+    import bench
+
+    root = Path(__file__).resolve().parent.parent
+    step = (root / "gpuwm-hex_b200" / "csrc" / "dycore_step.cuh").read_text()
+    labels = set(re.findall(r'\.lpvt?\("(k_[a-z0-9_]+)"', step))
+    labels |= set(re.findall(r'LPSN\(L, "(k_[a-z0-9_]+)"', step))
+    labels |= {x for pair in re.findall(r'"(k_[a-z0-9_]+)" : "(k_[a-z0-9_]+)"', step) for x in pair}
+    labels |= set(re.findall(r'LPG\(L, "(k_[a-z0-9_]+)"', step))
+    labels |= {"k_" + m for m in re.findall(r"LPST?\(L, [^,]+, [^,]+, ([a-z0-9_]+),", step)}
+    labels |= set(re.findall(r"LP\(L, [^,]+, [^,]+, [^,]+, (k_[a-z0-9_]+),", step))
+    labels -= {"k_name", "k_rebuild_cell", "k_recover_u"}  # macro text; the sidecar rebuild, not a step kernel
+    assert {"k_tend_u", "k_fct_cell2", "k_clamp_scalars", "k_mix_cell2", "k_diag_vertex"} <= labels
+    for name in sorted(labels):
+        assert bench.kernel_bytes(name, 10, 30, 20, 12, 3) > 0, name

@@ -239,7 +239,67 @@ def oracle_time_per_step(case, dt: float, budget_s: float, max_steps: int) -> tu
 
 
 def cores_used() -> int:
+    """Threads the CPU baseline computes on: the oracle is NumPy, whose
+    elementwise FP32 kernels run on the calling thread (the step uses no
+    BLAS), so one."""
     return 1
+
+
+def host_box() -> dict:
+    """The host the CPU baseline ran on: logical CPUs, the affinity mask the
+    process may use, and the thread-count variables that NumPy, BLAS and the
+    reference's host copy helpers read."""
+    try:
+        affinity = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        affinity = None
+    env = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                          "GPUWM_HEX_HOST_COPY_THREADS")}
+    cpu = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                cpu = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "affinity_cpus": affinity, "cpu": cpu, "env": env}
+
+
+CPU_PATH = ("the oracle: a vectorised NumPy FP32 restatement of the reference's DryDycoreDriver.step "
+            "(hexcore/driver.py:3314), bit-identical to it, single-threaded; the reference's own NumPy path "
+            "is also single-threaded and was 18x slower at 2562 cells")
+
+
+# Launch labels that run the same kernel function with other arguments.
+KERNEL_OF_LABEL = {"k_ac_edge_first": "kv_ac_edge", "k_ac_edge_damp": "kv_ac_edge", "k_ac_cell_first": "kv_ac_cell",
+                   "k_diag_edge_v": "kv_diag_edge", "k_tr_edge_mono": "kv_tr_edge"}
+
+
+def kernel_of(label: str) -> str:
+    """The kernel function a launch label runs (``k_x`` -> ``kv_x``)."""
+    return KERNEL_OF_LABEL.get(label, "kv_" + label[2:] if label.startswith("k_") else label)
+
+
+def by_kernel(kernels: dict, prof_steps: int) -> dict:
+    """Per-label profile entries merged per kernel function: launches, share,
+    average launch time and algorithmic bytes per launch (launch-weighted)."""
+    out: dict[str, dict] = {}
+    for label, k in kernels.items():
+        name = kernel_of(label)
+        n = k["launches_per_step"]
+        m = out.setdefault(name, {"labels": [], "launches_per_step": 0.0, "share": 0.0, "_us": 0.0, "_bytes": 0.0})
+        m["labels"].append(label)
+        m["launches_per_step"] += n
+        m["share"] += k["share"]
+        m["_us"] += k["avg_us"] * n
+        m["_bytes"] += (k["bytes"] or 0) * n
+    for m in out.values():
+        n = m["launches_per_step"]
+        m["avg_us"] = m.pop("_us") / n
+        m["bytes"] = m.pop("_bytes") / n
+        m["gbs"] = m["bytes"] / (m["avg_us"] * 1e-6) / 1e9 if m["bytes"] else None
+    return out
 
 
 # ------------------------------------------------------------- ensembles
@@ -398,7 +458,7 @@ def run_reference(args, rank: int) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args, case),
         "cpu_baseline": {"value": value, "unit": "simulated days/hour", "cores": cores_used(), "kind": "port",
-                         "sample": sample},
+                         "path": CPU_PATH, "host": host_box(), "sample": sample},
         "e2e": {"value": value, "unit": "simulated days/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -470,14 +530,20 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         kernels[name] = {"launches_per_step": n / prof_steps, "avg_us": avg_ms * 1000.0,
                          "share": ms / total_ms, "bytes": b,
                          "gbs": (b / (avg_ms / 1000.0) / 1e9) if b else None}
-    dominant = max(kernels, key=lambda k: kernels[k]["share"])
-    dk = kernels[dominant]
+    merged = by_kernel(kernels, prof_steps)
+    dominant = max(merged, key=lambda k: merged[k]["share"])
+    dk = merged[dominant]
     achieved = dk["gbs"]
     traffic = None
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         try:
-            traffic = json.loads(traffic_file.read_text()).get(dominant)
+            # ncu DRAM bytes per launch, per label; a kernel's is the
+            # launch-weighted mean over its labels (None unless all were captured)
+            known = json.loads(traffic_file.read_text())
+            if all(lb in known for lb in dk["labels"]):
+                traffic = sum(known[lb] * kernels[lb]["launches_per_step"] for lb in dk["labels"]) / \
+                    dk["launches_per_step"]
         except Exception:  # noqa: BLE001
             traffic = None
     step_bytes = sum(kernel_bytes(k, C, E, V, L, T) * kernels[k]["launches_per_step"] for k in kernels)
@@ -534,7 +600,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, n = oracle_time_per_step(case, dt, args.cpu_budget_s, 2)
         cpu = {"value": (dt / 86400.0) / (sec / 3600.0), "unit": "simulated days/hour", "cores": cores_used(),
-               "kind": "port",
+               "kind": "port", "path": CPU_PATH, "host": host_box(),
                "sample": f"{n} full large step(s) of this workload by the NumPy oracle (single thread), "
                          f"{sec:.1f} s/step"}
 
@@ -550,14 +616,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "gpu_launches": int(launches) * args.steps if not args.no_graph else int(launches) * args.steps,
             "gpu_launches_per_step": int(launches),
-            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+            "roofline": {"bound": "hbm", "kernel": dominant, "labels": dk["labels"], "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
                          "traffic": traffic, "bytes_per_launch": dk["bytes"], "avg_launch_us": dk["avg_us"],
                          "share": dk["share"]},
             "autotune": {k: v["threads"] for k, v in tuning.items()},
             "step_bytes_algorithmic": step_bytes,
             "step_gbs": step_bytes / (ms_per_step / 1000.0) / 1e9,
             "kernels": kernels,
+            "kernel_functions": merged,
             "batched": batched,
             "learned": learned,
             "cpu_baseline": cpu,

@@ -1675,15 +1675,11 @@ extern "C" int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, cons
   cudaStream_t st = (cudaStream_t)stream;
   const HexGeo& g = c.geo;
   const size_t CS = (size_t)g.nC * g.S, ES = (size_t)g.nE * g.S;
-  // what must start at zero (or one): the flag and the dry coefficients
-  HEX_CUDA(cudaMemsetAsync(c.w.flag, 0, sizeof(int), st), "clear flag");
-  if (g.smag_on) {
-    // the mixing arrays start cleared, as the allocating path's do
-    const size_t words = (size_t)(c.w.mix_w + CS - c.w.vorticity);
-    HEX_CUDA(cudaMemsetAsync(c.w.vorticity, 0, words * sizeof(float), st), "clear mixing");
-  }
+  // The array keeps the previous call's words (possibly of another mesh and
+  // layout): clear every word this step uses, as the allocating path's
+  // workspace starts cleared, then set what starts at one (dry coefficients).
+  HEX_CUDA(cudaMemsetAsync(base, 0, need, st), "clear no-alloc scratch");
   if (!g.moist) {
-    HEX_CUDA(cudaMemsetAsync(c.w.qtot, 0, CS * sizeof(float), st), "clear qtot");
     k_fill<<<(unsigned)((CS + 255) / 256), 256, 0, st>>>(c.w.cqw, CS, 1.0f);
     k_fill<<<(unsigned)((ES + 255) / 256), 256, 0, st>>>(c.w.cqu, ES, 1.0f);
     HEX_CUDA(cudaGetLastError(), "fill dry coefficients");

@@ -82,18 +82,32 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
 }
 
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
 // Bounded wait for the completion of phase `parity`; false when it gave up.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try(mbar, parity)) return true;
+  return false;
+}
+
+// As mbar_wait with at most `limit` polls, giving up early once another
+// role of the CTA has raised its abort word (checked every 64 polls).
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t mbar, uint32_t parity, volatile int* abort_word,
+                                                   uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (mbar_try(mbar, parity)) return true;
+    if ((i & 63u) == 63u && *abort_word) return false;
   }
   return false;
 }
@@ -165,6 +179,7 @@ struct Gemm {
   const bf16* Zin;
   float* Cf;
   int* err;
+  uint32_t mma_wait_polls;  // polls of the MMA issuer's wait for a loaded stage (WAIT_LIMIT normally)
 };
 
 // Epilogue of 8 accumulator columns of one row: bias, then the selected
@@ -344,7 +359,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
 // apply the epilogue and store, then release the accumulator.  The
 // epilogue of tile i thus overlaps the loads and MMAs of tile i+1.  Every
 // wait is bounded; a role that gives up raises the CTA's abort word and
-// all roles stop.
+// all roles stop.  Before the CTA frees its tensor memory and exits, the
+// producer waits for every TMA load it issued to land and the MMA issuer
+// commits a drain barrier and waits for every MMA it issued, so no
+// asynchronous copy or MMA is in flight at exit on either path.
 constexpr int WS_THREADS = 320;
 constexpr int WS_STAGES = 4;
 
@@ -384,7 +402,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   uint64_t* empty = full + WS_STAGES;
   uint64_t* acc_full = empty + WS_STAGES;
   uint64_t* acc_empty = acc_full + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  uint64_t* drain = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_word = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_n = p.N / BN, tiles = (p.M / BM) * n_n, nk = p.K / BK;
@@ -398,6 +417,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       mbar_init(smem_u32(&acc_full[i]), 1);
       mbar_init(smem_u32(&acc_empty[i]), 8);  // one arrival per epilogue warp
     }
+    mbar_init(smem_u32(drain), 1);
     *abort_word = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -415,11 +435,14 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     // TMA producer
     if (lane == 0) {
       int it = 0;
+      int last_it[WS_STAGES];  // last iteration whose loads went to each stage
+#pragma unroll
+      for (int s = 0; s < WS_STAGES; ++s) last_it[s] = -1;
       for (int t = blockIdx.x; t < tiles && !*abort_word; t += gridDim.x) {
         const int m0 = (t / n_n) * BM, n0 = (t % n_n) * BN;
         for (int kt = 0; kt < nk; ++kt, ++it) {
           const int s = it % WS_STAGES;
-          if (!mbar_wait(smem_u32(&empty[s]), ((it / WS_STAGES) & 1) ^ 1)) {
+          if (!mbar_wait_or_abort(smem_u32(&empty[s]), ((it / WS_STAGES) & 1) ^ 1, abort_word, WAIT_LIMIT)) {
             *abort_word = 1;
             break;
           }
@@ -427,8 +450,15 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           mbar_expect_tx(smem_u32(&full[s]), STAGE);
           tma_load_2d(smem_u32(a), &tmA, kt * BK, m0, smem_u32(&full[s]));
           tma_load_2d(smem_u32(a + A_BYTES), &tmB, kt * BK, n0, smem_u32(&full[s]));
+          last_it[s] = it;
         }
       }
+      // Every load issued has landed before the stage memory may go away:
+      // the last load into stage s completes phase last_it[s] / WS_STAGES of
+      // full[s], and no later load can move that barrier on.
+#pragma unroll
+      for (int s = 0; s < WS_STAGES; ++s)
+        if (last_it[s] >= 0 && !mbar_wait(smem_u32(&full[s]), (last_it[s] / WS_STAGES) & 1)) *abort_word = 1;
     }
   } else if (warp == 1) {
     // MMA issuer
@@ -437,7 +467,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       int it = 0, tc = 0;
       for (int t = blockIdx.x; t < tiles && !*abort_word; t += gridDim.x, ++tc) {
         const int b = tc & 1;
-        if (!mbar_wait(smem_u32(&acc_empty[b]), ((tc >> 1) & 1) ^ 1)) {
+        if (!mbar_wait_or_abort(smem_u32(&acc_empty[b]), ((tc >> 1) & 1) ^ 1, abort_word, WAIT_LIMIT)) {
           *abort_word = 1;
           break;
         }
@@ -445,7 +475,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         const uint32_t acc = tmem + (uint32_t)(b * BN);
         for (int kt = 0; kt < nk; ++kt, ++it) {
           const int s = it % WS_STAGES;
-          if (!mbar_wait(smem_u32(&full[s]), (it / WS_STAGES) & 1)) {
+          if (!mbar_wait_or_abort(smem_u32(&full[s]), (it / WS_STAGES) & 1, abort_word, p.mma_wait_polls)) {
             *abort_word = 1;
             break;
           }
@@ -460,6 +490,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         if (*abort_word) break;
         mma_commit(smem_u32(&acc_full[b]));
       }
+      // Every MMA issued by this thread completes before the tensor memory
+      // and the stage buffers it reads may be released.
+      mma_commit(smem_u32(drain));
+      if (!mbar_wait(smem_u32(drain), 0)) *abort_word = 1;
     }
   } else {
     // epilogue warps 2..9: lane quarter warp % 4, column half (warp - 2) / 4
@@ -468,7 +502,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tc) {
       const int b = tc & 1;
       bool ok = true;
-      if (lane == 0) ok = mbar_wait(smem_u32(&acc_full[b]), (tc >> 1) & 1);
+      if (lane == 0) ok = mbar_wait_or_abort(smem_u32(&acc_full[b]), (tc >> 1) & 1, abort_word, WAIT_LIMIT);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) {
         if (lane == 0) *abort_word = 1;
@@ -491,12 +525,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     }
   }
   __syncthreads();
-  if (*abort_word) {
-    if (threadIdx.x == 0) atomicOr(p.err, 1);
-    // bounded wait for the last accumulator commit of each buffer still in flight
-    if (threadIdx.x == 32)
-      for (int b = 0; b < 2; ++b) mbar_wait(smem_u32(&acc_full[b]), 0);
-  }
+  if (*abort_word && threadIdx.x == 0) atomicOr(p.err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -655,9 +684,9 @@ int launch_ws(const Gemm& g, cudaStream_t st) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
+int gemm_impl(const HexMlpGemm* p, uint32_t mma_wait_polls, void* stream) {
   if (!p || !p->A || !p->B || !p->err) return HEXMLP_E_ARG;
   if (p->M <= 0 || p->N <= 0 || p->K <= 0 || p->M % BM || p->K % BK) return HEXMLP_E_ARG;
   if (!(p->bn == 128 || p->bn == 256) || p->N % p->bn) return HEXMLP_E_ARG;
@@ -673,13 +702,24 @@ int hexmlp_gemm(const HexMlpGemm* p, void* stream) {
   cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return (int)e;
   const Gemm g{(const bf16*)p->A, (const bf16*)p->B, p->M, p->N, p->K, p->bn, p->epilogue, p->bias, (bf16*)p->C,
-               (bf16*)p->Ct, (bf16*)p->Z, (const bf16*)p->Zin, p->Cf, p->err};
+               (bf16*)p->Ct, (bf16*)p->Z, (const bf16*)p->Zin, p->Cf, p->err, mma_wait_polls};
   if (p->kernel == HEXMLP_GEMM_PERSISTENT)
     return p->bn == 256 ? launch_ws<256>(g, (cudaStream_t)stream) : launch_ws<128>(g, (cudaStream_t)stream);
-  if (p->kernel != HEXMLP_GEMM_STAGED) return HEXMLP_E_ARG;
+  if (p->kernel != HEXMLP_GEMM_STAGED || mma_wait_polls != WAIT_LIMIT) return HEXMLP_E_ARG;
   dim3 grid(p->M / BM, p->N / p->bn);
   k_gemm_bf16<<<grid, THREADS, smem, (cudaStream_t)stream>>>(g);
   return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+int hexmlp_gemm(const HexMlpGemm* p, void* stream) { return gemm_impl(p, WAIT_LIMIT, stream); }
+
+int hexmlp_gemm_wait_limit(const HexMlpGemm* p, uint32_t mma_wait_polls, void* stream) {
+  if (!p || p->kernel != HEXMLP_GEMM_PERSISTENT) return HEXMLP_E_ARG;
+  return gemm_impl(p, mma_wait_polls, stream);
 }
 
 int hexmlp_mse_grad(const float* Y, const float* T, int M, int N, int m_valid, int n_valid, float scale,

@@ -30,6 +30,78 @@ def _refuse(knob: str, value: object, reason: str, declaration: str) -> None:
     raise ConfigurationRefusal(knob, value, reason, declaration)
 
 
+# Knobs of the reference's configuration classes that this path does not
+# implement, with the reference's defaults and why each is refused when set
+# to anything else: ``V841DryDycoreConfig`` (hexcore/config_v841.py:114-140)
+# and its base ``DryDycoreConfig`` (hexcore/driver.py:172-260).
+UNMODELLED_REFERENCE_KNOBS: dict[str, tuple[object, str]] = {
+    "config_physics_suite": ("none", "physics suites run outside the dycore step"),
+    "config_iau_option": ("off", "incremental analysis update forcing is not part of this step"),
+    "config_h_theta_eddy_visc2": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_v_theta_eddy_visc2": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_h_mom_eddy_visc2": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_v_mom_eddy_visc2": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_h_theta_eddy_visc4": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_h_mom_eddy_visc4": (0.0, "fixed eddy viscosities (2d_fixed mixing) are not implemented"),
+    "config_vertical_mixing": (False, "the saved vertical Euler filters are not implemented"),
+    "config_curvature_terms": (False, "the optional curvature branch is not implemented"),
+    "config_gpu_aware_mpi": (False, "this path has no MPI transport"),
+    "config_les_model": ("none", "LES / 3-D Smagorinsky mixing is not implemented"),
+    "config_les_surface": ("none", "LES surface forcing is not implemented"),
+    "config_mix_scalars": (False, "3-D mixing of scalars is not implemented"),
+    "config_mix_full": (True, "the 3-D mixing variants are not implemented"),
+    "config_surface_heat_flux": (0.0, "prescribed surface fluxes belong to the LES branch, not implemented"),
+    "config_surface_moisture_flux": (0.0, "prescribed surface fluxes belong to the LES branch, not implemented"),
+    "config_surface_drag_coefficient": (0.0, "prescribed surface drag belongs to the LES branch, not implemented"),
+    "source_release": ("v8.4.1", "this path implements the v8.4.1/8.4.2 numerics"),
+}
+
+
+def _refuse_unmodelled(config: Any, modelled: set[str]) -> None:
+    """Refuse, by name, every knob of a reference configuration that this
+    path does not model and whose value is not the reference's default.
+    Dataclass configurations are checked field by field against their own
+    defaults (so knobs added to the reference later are caught too); other
+    objects against ``UNMODELLED_REFERENCE_KNOBS``."""
+    defaults: dict[str, object] = {}
+    try:
+        import dataclasses
+
+        for f in dataclasses.fields(config):
+            if f.default is not dataclasses.MISSING:
+                defaults[f.name] = f.default
+            elif f.default_factory is not dataclasses.MISSING:  # type: ignore[misc]
+                defaults[f.name] = f.default_factory()  # type: ignore[misc]
+    except TypeError:
+        pass
+    for knob, (default, _) in UNMODELLED_REFERENCE_KNOBS.items():
+        defaults.setdefault(knob, default)
+    for knob, default in defaults.items():
+        if knob in modelled or not hasattr(config, knob):
+            continue
+        value = getattr(config, knob)
+        if knob == "config_terrain_following":
+            # hexcore/driver.py:2286-2305: True or None run with the terrain
+            # metrics this path always takes; False would drop them
+            if value is False:
+                _refuse(knob, value, "this path always applies the native terrain metrics",
+                        "config_terrain_following=True or None")
+            continue
+        if knob == "source_release":
+            default = UNMODELLED_REFERENCE_KNOBS[knob][0]
+        if isinstance(default, bool) or isinstance(value, bool):
+            same = type(value) is type(default) and value == default
+        else:
+            try:
+                same = bool(value == default)
+            except Exception:  # noqa: BLE001
+                same = False
+        if not same:
+            reason = UNMODELLED_REFERENCE_KNOBS.get(knob, (None, "this knob is not implemented on the GPU step "
+                                                                 "path"))[1]
+            _refuse(knob, value, reason, f"{knob}={default!r}")
+
+
 @dataclass(frozen=True)
 class DycoreConfig:
     """The v8.4.1/8.4.2 dry-plus-tracer lane on one GPU."""
@@ -99,7 +171,12 @@ class DycoreConfig:
     @classmethod
     def from_reference(cls, config: Any, **overrides: Any) -> "DycoreConfig":
         """Project a reference ``V841DryDycoreConfig`` (or any object with the
-        same attribute names) onto this configuration."""
+        same attribute names) onto this configuration.  Every reference knob
+        this path does not model must hold the reference's default; any other
+        value is refused by name (``ConfigurationRefusal``) before any device
+        work, as ``hexcore/cuda_driver.py:3096-3215`` refuses before launching."""
+        modelled = {f.name for f in fields(cls)}
+        _refuse_unmodelled(config, modelled)
         values = {f.name: getattr(config, f.name) for f in fields(cls) if hasattr(config, f.name)}
         values.update(overrides)
         out = cls(**values)

@@ -169,6 +169,22 @@ def average_gradients(tensors, group=None) -> None:
         t.div_(world)
 
 
+def global_mean_loss(loss_sum: float, count: int, group=None) -> float:
+    """An epoch's mean training loss over every rank of ``group`` (the
+    summed squared errors and the element counts are all-reduced together),
+    so every rank records the loss of the global batch sequence; without a
+    group, the local mean."""
+    if group is None:
+        return loss_sum / max(count, 1)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([loss_sum, float(count)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return float(t[0].item()) / max(float(t[1].item()), 1.0)
+
+
 def _stats(x: np.ndarray, floor: float = 1e-12):
     mean = x.mean(axis=0).astype(np.float32)
     std = x.std(axis=0).astype(np.float32)
@@ -201,8 +217,11 @@ class TrainedNet:
         same split and initial weights) each rank runs its shard of every
         epoch's batches and the weight and bias gradients are averaged over
         the ranks before each optimizer step, so the weights stay identical
-        on every rank (data parallel).  Without a group the rank trains
-        alone."""
+        on every rank (data parallel).  Each epoch runs
+        ``(n_batches // W) * W`` batches, so with W > 1 up to W - 1 full
+        batches of a reshuffled epoch are left out (a different set each
+        epoch); ``train_loss`` is the mean over all ranks' batches.  Without a
+        group the rank trains alone."""
         import torch
         import torch.distributed as dist
 
@@ -272,7 +291,7 @@ class TrainedNet:
                 rec.steps += 1
                 ep_loss += float(loss.item())
                 ep_n += n * self.n_out
-            rec.train_loss.append(ep_loss / max(ep_n, 1))
+            rec.train_loss.append(global_mean_loss(ep_loss, ep_n, group if world > 1 else None))
         torch.cuda.synchronize()
         rec.seconds = time.perf_counter() - t0
         net.check()

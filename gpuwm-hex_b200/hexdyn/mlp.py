@@ -36,6 +36,7 @@ GEMM_PERSISTENT, GEMM_STAGED = 0, 1
 
 MLP_EXPORTS = {
     "hexmlp_gemm": (C.c_int, [C.POINTER(HexMlpGemm), C.c_void_p]),
+    "hexmlp_gemm_wait_limit": (C.c_int, [C.POINTER(HexMlpGemm), C.c_uint32, C.c_void_p]),
     "hexmlp_gemm_smem_bytes": (C.c_size_t, [C.c_int]),
     "hexmlp_gemm_tile_rows": (C.c_int, []),
     "hexmlp_gemm_tile_k": (C.c_int, []),
@@ -81,10 +82,12 @@ def round_up(x: int, m: int) -> int:
 
 
 def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=None, Zin=None, Cf=None, err=None,
-         bn: int | None = None, kernel: int = GEMM_PERSISTENT):
+         bn: int | None = None, kernel: int = GEMM_PERSISTENT, mma_wait_polls: int | None = None):
     """C = A . B^T on the tensor cores (see include/hexmlp.h).  ``bn``: the
     output tile width, 128 or 256 (default: 256 where N allows it for the
-    persistent kernel, 128 for the staged one)."""
+    persistent kernel, 128 for the staged one).  ``mma_wait_polls`` bounds
+    the MMA issuer's wait for each loaded stage (``hexmlp_gemm_wait_limit``,
+    a check of the kernel's give-up path; None: the normal limit)."""
     import torch
 
     M, K = A.shape
@@ -97,7 +100,11 @@ def gemm(A, B, *, epilogue: int = EPI_F32, bias=None, C_out=None, Ct=None, Z=Non
         bn = 256 if (kernel == GEMM_PERSISTENT and N % 256 == 0) else 128
     p = HexMlpGemm(_ptr(A), _ptr(B), M, N, K, bn, epilogue, _ptr(bias), _ptr(C_out), _ptr(Ct), _ptr(Z), _ptr(Zin),
                    _ptr(Cf), _ptr(err), kernel)
-    _check(load().hexmlp_gemm(C.byref(p), _stream()), f"hexmlp_gemm {M}x{N}x{K}")
+    if mma_wait_polls is None:
+        _check(load().hexmlp_gemm(C.byref(p), _stream()), f"hexmlp_gemm {M}x{N}x{K}")
+    else:
+        _check(load().hexmlp_gemm_wait_limit(C.byref(p), int(mma_wait_polls), _stream()),
+               f"hexmlp_gemm_wait_limit {M}x{N}x{K}")
     return err
 
 

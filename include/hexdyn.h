@@ -254,24 +254,26 @@ typedef struct HexDynFields {
 int hexdyn_bind_state(HexDynHandle* h, const HexDynFields* fields, void* stream);
 
 /* No counterpart in the reference: one large step that allocates nothing.
- * For callers that cannot call cudaMalloc when they step -- code running
- * while its own stream is being captured into a CUDA graph (an allocation
- * there breaks the capture), host frameworks whose device memory is owned by
- * a pool that must not be bypassed, or ensembles that keep every member's
- * state in their own buffers and cannot give each member a private
- * workspace.  The caller passes the input state and sidecar and the output
- * buffers (`in` and `out` must not overlap); the mesh comes from `h`.  Every
- * intermediate of the step (tendencies, acoustic perturbations, coefficients,
- * subcycle states, transport limiter fields) lives in one file-scope device
- * array of 64 MiB that each GPU loading the library holds until exit; a step
- * needing more returns HEXDYN_E_CAPACITY and names the size.  The first call
- * on a device looks up that array's address (cudaGetSymbolAddress) and must
- * come before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (different streams, or concurrent host threads) race on
- * it, so issue them on one stream.  Each call clears what must start at zero
- * (the validation flag and the dry moist-coefficient fields) and writes every
- * other scratch word before reading it.  Reads the flag at the end like
- * hexdyn_step (synchronises `stream`). */
+ * For callers that cannot call cudaMalloc when they step -- host frameworks
+ * whose device memory is owned by a pool that must not be bypassed (an
+ * allocation outside it breaks their accounting or fails under their memory
+ * limit), or ensembles that keep every member's state in their own buffers
+ * and cannot give each member a private workspace.  The caller passes the
+ * input state and sidecar and the output buffers (`in` and `out` must not
+ * overlap); the mesh and configuration come from `h`.  Every intermediate of
+ * the step (tendencies, acoustic perturbations, coefficients, subcycle
+ * states, transport limiter fields) lives in one file-scope device array of
+ * 64 MiB that each GPU loading the library holds until exit; a step needing
+ * more returns HEXDYN_E_CAPACITY and names the size (2562 cells x 55 levels
+ * with 6 scalars is already too large).  The first call on a device looks up
+ * that array's address (cudaGetSymbolAddress, with that device current, in
+ * its primary context).  All calls share the array and it keeps the last
+ * call's contents: each call clears the words it uses before the step, and
+ * calls that overlap on the GPU (different streams, or concurrent host
+ * threads) race on it, so issue them on one stream.  Kernels run on `stream`
+ * alone (no second stream) at 256 threads per block (the handle's autotuned
+ * block sizes are not used).  Reads the flag at the end like hexdyn_step
+ * (synchronises `stream`). */
 int hexdyn_step_noalloc(HexDynHandle* h, const HexDynFields* in, const HexDynFields* out, void* stream,
                         int* flag_out);
 

@@ -54,6 +54,13 @@ typedef struct HexMlpGemm {
 #define HEXMLP_GEMM_STAGED 1
 
 int hexmlp_gemm(const HexMlpGemm* p, void* stream);
+/* Check of the persistent GEMM's failure path: hexmlp_gemm with the MMA
+ * issuer's wait for each loaded stage bounded by `mma_wait_polls` mbarrier
+ * polls instead of 2^20.  With 0 that wait gives up before the first stage
+ * lands: the kernel sets *err, its producer waits for every TMA load it
+ * issued, its MMA issuer for every MMA it issued, it frees its tensor memory
+ * and returns (outputs invalid).  Only HEXMLP_GEMM_PERSISTENT. */
+int hexmlp_gemm_wait_limit(const HexMlpGemm* p, uint32_t mma_wait_polls, void* stream);
 size_t hexmlp_gemm_smem_bytes(int bn);
 int hexmlp_gemm_tile_rows(void);
 int hexmlp_gemm_tile_k(void);

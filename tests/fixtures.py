@@ -2,6 +2,8 @@
 
 from __future__ import annotations
 
+import hashlib
+import json
 from pathlib import Path
 from types import SimpleNamespace
 
@@ -11,6 +13,7 @@ from hexdyn.case import VerticalGridData
 from hexdyn.mesh import VoronoiMesh
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
+REPO = Path(__file__).resolve().parent.parent
 STATE = ("rho", "rho_theta", "rho_u", "rho_w", "scalars")
 SIDE = ("theta_m", "exner", "density_perturbation", "rho_theta_perturbation",
         "pressure_perturbation", "normal_velocity", "vertical_velocity")
@@ -46,6 +49,65 @@ VARIANTS = [("l2_L12_sub1", 2), ("l2_L12_sub4", 2), ("l2_L12_nomono", 2), ("l2_L
             ("l2_L12_smag", 2)]
 
 
+# The 162-cell case with qv + 5 condensates and the same inputs cut to 4 and 5
+# scalars: (name, steps); each fixture holds dry and native-moist outputs.
+SCALAR_VARIANTS = [("l2_L12_t6", 2), ("l2_L12_t5", 2), ("l2_L12_t4", 2)]
+
+
+def array_digest(a) -> str:
+    """SHA-256 of an array's dtype, shape and C-order bytes."""
+    a = np.ascontiguousarray(a)
+    h = hashlib.sha256(f"{a.dtype.str}{a.shape}".encode())
+    h.update(a.tobytes())
+    return h.hexdigest()
+
+
+def inputs_digest(arrays: dict) -> str:
+    """One SHA-256 over every input array (case arrays), in name order."""
+    h = hashlib.sha256()
+    for k in sorted(arrays):
+        h.update(k.encode())
+        h.update(array_digest(arrays[k]).encode())
+    return h.hexdigest()
+
+
+def load_digests(name: str) -> dict:
+    """A digest record of the reference's outputs at full size
+    (tests/golden/digests_<name>.json)."""
+    path = GOLDEN / f"digests_{name}.json"
+    if not path.exists():
+        import pytest
+
+        pytest.skip(f"{path.name} has not been generated (tests/golden/make_golden.py REFERENCE_ROOT {name})")
+    return json.loads(path.read_text())
+
+
+def digest_case(record: dict):
+    """The case a digest record was made from, rebuilt here, and whether its
+    inputs carry the recorded digest (NumPy's SIMD transcendental paths
+    depend on the host CPU, so another host may build other bits)."""
+    from hexdyn.case import build_case, case_arrays
+    from hexdyn.mesh import build_mesh
+
+    c = record["case"]
+    mesh = build_mesh(c["mesh_level"], lloyd=c["lloyd"], seed=c["seed"])
+    arr = case_arrays(build_case(mesh, n_levels=c["levels"], seed=c["seed"], n_condensates=c["condensates"]))
+    return arr, inputs_digest(arr) == record["inputs_sha256"]
+
+
+def mismatched_digests(record: dict, label: str, step: int, state, side) -> list:
+    """Names of the fields of one step whose words differ from the record."""
+    bad = []
+    for k in STATE:
+        if array_digest(np.asarray(getattr(state, k), dtype=np.float32)) != record["outputs"][f"{label}.step{step}.{k}"]:
+            bad.append(k)
+    for k in SIDE:
+        got = array_digest(np.asarray(getattr(side, k), dtype=np.float32))
+        if got != record["outputs"][f"{label}.step{step}.side.{k}"]:
+            bad.append(k)
+    return bad
+
+
 def inputs(fx: dict) -> dict:
     """The case arrays (``hexdyn.case.case_arrays`` layout) of a fixture."""
     return {k[3:]: v for k, v in fx.items() if k.startswith("in.")}
@@ -73,3 +135,47 @@ def differing_words(a, b) -> int:
     b = np.ascontiguousarray(b, dtype=np.float32)
     assert a.shape == b.shape, (a.shape, b.shape)
     return int(np.count_nonzero(a.view(np.uint32) != b.view(np.uint32)))
+
+
+def reference_stub_dir() -> str:
+    """A temporary directory holding a two-class ``netCDF4`` stub and a
+    ``gpuwm`` stub: the reference's dycore modules import them at module
+    level for file I/O and LES route checks only."""
+    import tempfile
+
+    d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
+    (d / "netCDF4").mkdir()
+    (d / "netCDF4" / "__init__.py").write_text(
+        "class Dataset:\n    def __init__(self, *a, **k):\n        raise RuntimeError('no netCDF I/O')\n"
+        "class Variable:\n    pass\n")
+    (d / "gpuwm").mkdir()
+    (d / "gpuwm" / "__init__.py").write_text("")
+    (d / "gpuwm" / "backend.py").write_text(
+        "def compilation_target(*a, **k):\n    raise RuntimeError('no gpuwm')\n")
+    return str(d)
+
+
+def reference_root():
+    """The reference checkout: ``HEXDYN_REFERENCE_ROOT``, else a ``reference``
+    directory beside this repository; None when neither holds the sources."""
+    import os
+
+    for cand in (os.environ.get("HEXDYN_REFERENCE_ROOT"), str(REPO.parent / "reference")):
+        if cand and (Path(cand) / "tree" / "src" / "hexcore").is_dir():
+            return Path(cand)
+    return None
+
+
+def import_reference():
+    """Put the reference's sources (and the stubs) on ``sys.path``; returns
+    the root, or None when the checkout is absent."""
+    import sys
+
+    root = reference_root()
+    if root is None:
+        return None
+    src = str(root / "tree" / "src")
+    if src not in sys.path:
+        sys.path.insert(0, reference_stub_dir())
+        sys.path.insert(0, src)
+    return root

@@ -3,8 +3,17 @@
 Runs the reference's CPU dycore authority (``hexcore.driver.DryDycoreDriver``
 with ``V841DryDycoreConfig``, gpuwm-hex 0.5.0) on small synthetic cases built
 by ``hexdyn.case`` and stores inputs and outputs as ``.npz`` fixtures.  It
-needs the reference checkout (default ``/root/reference``) and therefore runs
-only where that exists; the fixtures it writes are what the tests read.
+needs the reference checkout, given as the first argument or in the
+``HEXDYN_REFERENCE_ROOT`` environment variable, and therefore runs only where
+that exists; the fixtures it writes are what the tests read.
+
+At the two large sizes (2562 cells x 55 levels with qv; 40962 cells x 55
+levels with qv and 5 condensates, the throughput workload) it stores SHA-256
+digests of every input array and every output field instead of the arrays
+(``digests_<name>.json``): the inputs are rebuilt by ``hexdyn.case`` where the
+tests run, and a test compares digests only where the rebuilt inputs have the
+recorded digest (NumPy's transcendental functions take SIMD paths that depend
+on the host CPU, so another host may build other input bits).
 
 Harness: a two-class ``netCDF4`` stub and a ``gpuwm``
 stub are put on ``sys.path`` (the reference imports them only for file I/O
@@ -15,11 +24,15 @@ case builder.  The ``native`` fixture wraps the driver so that
 carried scalar (``hexcore/regional_v841.py:1180``), which is what native MPAS
 and the reference's CUDA driver apply with physics off.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference [fixture names ...]]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT [fixture names ...]
+       HEXDYN_REFERENCE_ROOT=... python tests/golden/make_golden.py [fixture names ...]
 """
 
 from __future__ import annotations
 
+import hashlib
+import json
+import os
 import sys
 import tempfile
 import time
@@ -30,14 +43,33 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT / "gpuwm-hex_b200"))
+sys.path.insert(0, str(HERE.parent))
 
+from fixtures import array_digest, inputs_digest, reference_stub_dir  # noqa: E402
 from hexdyn.case import build_case, case_arrays  # noqa: E402
 from hexdyn.mesh import build_mesh  # noqa: E402
 
 CASES = {
-    # name: (mesh level, levels, condensates, dt, sub steps, steps, native moist)
-    "l2_L12": (2, 12, 1, 1800.0, 2, 2, True),
-    "l3_L20": (3, 20, 0, 1800.0, 2, 1, False),
+    # name: (mesh level, levels, condensates, dt, sub steps, steps, native moist steps)
+    "l2_L12": (2, 12, 1, 1800.0, 2, 2, 1),
+    "l3_L20": (3, 20, 0, 1800.0, 2, 1, 0),
+    # qv + 5 condensates, the tracer count of the throughput workload
+    "l2_L12_t6": (2, 12, 5, 1800.0, 2, 2, 2),
+}
+
+# The same inputs with the first 4 and 5 scalars only (every scalar count
+# from 4 to 6 then has reference outputs): name -> (base, scalars kept,
+# steps); both moist-coefficient semantics.
+SCALAR_VARIANTS = {
+    "l2_L12_t4": ("l2_L12_t6", 4, 2),
+    "l2_L12_t5": ("l2_L12_t6", 5, 2),
+}
+
+# Digest-only runs at full size, native moist coefficients:
+# name -> (mesh level, levels, condensates, dt, sub steps, steps)
+DIGESTS = {
+    "c1": (4, 55, 0, 1800.0, 2, 2),
+    "c2": (6, 55, 5, 720.0, 2, 1),
 }
 
 # Configuration variants on the inputs of a base case (outputs only; the
@@ -63,21 +95,10 @@ SMAG_VARIANTS = {
 }
 
 
-def _stubs() -> str:
-    d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
-    (d / "netCDF4").mkdir()
-    (d / "netCDF4" / "__init__.py").write_text(
-        "class Dataset:\n    def __init__(self, *a, **k):\n        raise RuntimeError('no netCDF I/O')\n"
-        "class Variable:\n    pass\n")
-    (d / "gpuwm").mkdir()
-    (d / "gpuwm" / "__init__.py").write_text("")
-    (d / "gpuwm" / "backend.py").write_text(
-        "def compilation_target(*a, **k):\n    raise RuntimeError('no gpuwm')\n")
-    return str(d)
-
-
-def main(reference_root: str = "/root/reference", *only: str) -> None:
-    sys.path.insert(0, _stubs())
+def main(reference_root: str, *only: str) -> None:
+    if not (Path(reference_root) / "tree" / "src" / "hexcore").is_dir():
+        raise SystemExit(f"{reference_root!r} holds no tree/src/hexcore: give the reference checkout")
+    sys.path.insert(0, reference_stub_dir())
     sys.path.insert(0, str(Path(reference_root) / "tree" / "src"))
     from hexcore.config_v841 import V841DryDycoreConfig
     from hexcore.driver import DryDycoreDriver, DryReferenceState, TerrainMetrics
@@ -113,30 +134,59 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
                       "pressure_perturbation", "normal_velocity", "vertical_velocity"):
                 out[f"{label}.step{step}.side.{k}"] = np.asarray(getattr(side, k))
 
-    for name, (level, nlev, ncond, dt, nsub, nsteps, native) in CASES.items():
-        if only and name not in only and not any(v[0] == name for k, v in {**VARIANTS, **SMAG_VARIANTS}.items()
-                                                 if k in only):
-            continue
-        t0 = time.time()
-        mesh = build_mesh(level, lloyd=20, seed=0)
-        case = build_case(mesh, n_levels=nlev, seed=0, n_condensates=ncond)
+    def reference_inputs(case):
         vg = VerticalGrid(**{k: getattr(case.vertical, k) for k in case.vertical.__dataclass_fields__})
         ref = DryReferenceState(case.rho_base, case.rho_theta_base, case.pressure_base, case.exner_base)
         tm = TerrainMetrics(case.zb_cell, case.zb3_cell)
         ac = AdvectionCoefficients(case.adv_coefs, case.adv_coefs_3rd, case.n_adv_cells_for_edge,
                                    case.adv_cells_for_edge, 3, None)
         wp = V841ReferenceWindProfiles(case.u_init, case.v_init)
-        cfg = V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, config_dynamics_split_steps=3,
-                                  config_split_dynamics_transport=True, config_monotonic=True,
-                                  config_positive_definite=False, config_coef_3rd_order=0.25,
-                                  config_apvm_upwinding=0.5)
+        return vg, ref, ac, tm, wp
+
+    def base_config(dt, nsub):
+        return V841DryDycoreConfig(config_dt=dt, config_number_of_sub_steps=nsub, config_dynamics_split_steps=3,
+                                   config_split_dynamics_transport=True, config_monotonic=True,
+                                   config_positive_definite=False, config_coef_3rd_order=0.25,
+                                   config_apvm_upwinding=0.5)
+
+    for name, (level, nlev, ncond, dt, nsub, nsteps) in DIGESTS.items():
+        if name not in only:  # minutes to hours of CPU: only on request
+            continue
+        t0 = time.time()
+        mesh = build_mesh(level, lloyd=20, seed=0)
+        case = build_case(mesh, n_levels=nlev, seed=0, n_condensates=ncond)
+        arrays = case_arrays(case)
+        vg, ref, ac, tm, wp = reference_inputs(case)
+        out = {}
+        run(NativeMoistDriver, mesh, vg, ref, base_config(dt, nsub), ac, tm, wp, case, nsteps, "native", out)
+        record = {"case": {"mesh_level": level, "lloyd": 20, "seed": 0, "levels": nlev, "condensates": ncond,
+                           "dt": dt, "sub_steps": nsub, "steps": nsteps, "moist_coefficients": "native"},
+                  "made_by": "hexcore.driver.DryDycoreDriver (V841DryDycoreConfig), native moist coefficients",
+                  "inputs_sha256": inputs_digest(arrays),
+                  "inputs": {k: array_digest(v) for k, v in sorted(arrays.items())},
+                  "outputs": {k: array_digest(v) for k, v in sorted(out.items())},
+                  "reference_seconds": round(time.time() - t0, 1)}
+        path = HERE / f"digests_{name}.json"
+        path.write_text(json.dumps(record, indent=1) + "\n")
+        print(f"{path.name}: {len(out)} output digests in {time.time() - t0:.1f}s")
+
+    variants = {**VARIANTS, **SMAG_VARIANTS, **SCALAR_VARIANTS}
+    for name, (level, nlev, ncond, dt, nsub, nsteps, native_steps) in CASES.items():
+        if only and name not in only and not any(v[0] == name for k, v in variants.items() if k in only):
+            continue
+        t0 = time.time()
+        mesh = build_mesh(level, lloyd=20, seed=0)
+        case = build_case(mesh, n_levels=nlev, seed=0, n_condensates=ncond)
+        vg, ref, ac, tm, wp = reference_inputs(case)
+        cfg = base_config(dt, nsub)
         out = {f"in.{k}": v for k, v in case_arrays(case).items()}
         out["config.dt"] = dt
         out["config.n_sub_steps"] = nsub
         if not only or name in only:
-            runs = [("dry", DryDycoreDriver)] + ([("native", NativeMoistDriver)] if native else [])
-            for label, cls in runs:
-                run(cls, mesh, vg, ref, cfg, ac, tm, wp, case, nsteps if label == "dry" else 1, label, out)
+            runs = [("dry", DryDycoreDriver, nsteps)] + ([("native", NativeMoistDriver, native_steps)]
+                                                         if native_steps else [])
+            for label, cls, n in runs:
+                run(cls, mesh, vg, ref, cfg, ac, tm, wp, case, n, label, out)
             path = HERE / f"step_{name}.npz"
             np.savez_compressed(path, **out)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
@@ -196,7 +246,28 @@ def main(reference_root: str = "/root/reference", *only: str) -> None:
             path = HERE / f"step_{vname}.npz"
             np.savez_compressed(path, **vout)
             print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
+        for vname, (base, keep, vsteps) in SCALAR_VARIANTS.items():
+            if base != name or (only and vname not in only):
+                continue
+            import dataclasses
+
+            t0 = time.time()
+            vcase = dataclasses.replace(case, scalars=case.scalars[:keep].copy())
+            vout = {"base": np.array(base), "config.dt": dt, "config.n_sub_steps": nsub, "config.n_scalars": keep}
+            run(DryDycoreDriver, mesh, vg, ref, cfg, ac, tm, wp, vcase, vsteps, "dry", vout)
+            run(NativeMoistDriver, mesh, vg, ref, cfg, ac, tm, wp, vcase, vsteps, "native", vout)
+            path = HERE / f"step_{vname}.npz"
+            np.savez_compressed(path, **vout)
+            print(f"{path.name}: {path.stat().st_size / 1e6:.2f} MB in {time.time() - t0:.1f}s")
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    args = sys.argv[1:]
+    env_root = os.environ.get("HEXDYN_REFERENCE_ROOT")
+    if args and (Path(args[0]) / "tree").is_dir():
+        root, names = args[0], args[1:]
+    elif env_root:
+        root, names = env_root, args
+    else:
+        raise SystemExit("usage: make_golden.py REFERENCE_ROOT [names...] (or set HEXDYN_REFERENCE_ROOT)")
+    main(root, *names)

@@ -87,3 +87,25 @@ def test_bench_byte_model_covers_every_step_kernel():
     assert {"k_tend_u", "k_fct_cell2", "k_clamp_scalars", "k_mix_cell2", "k_diag_vertex"} <= labels
     for name in sorted(labels):
         assert bench.kernel_bytes(name, 10, 30, 20, 12, 3) > 0, name
+
+
+def test_bench_roofline_merges_labels_of_one_kernel():
+    """The roofline names a kernel function: launch labels that run the same
+    function (the first acoustic substep's k_ac_cell_first and the later
+    k_ac_cell) are merged, shares added, time and bytes launch-weighted."""
+    import bench
+
+    kernels = {"k_ac_cell_first": {"launches_per_step": 9, "avg_us": 80.0, "share": 0.09, "bytes": 200e6},
+               "k_ac_cell": {"launches_per_step": 3, "avg_us": 90.0, "share": 0.035, "bytes": 260e6},
+               "k_tend_u": {"launches_per_step": 9, "avg_us": 92.0, "share": 0.105, "bytes": 159e6}}
+    merged = bench.by_kernel(kernels, 1)
+    assert set(merged) == {"kv_ac_cell", "kv_tend_u"}
+    ac = merged["kv_ac_cell"]
+    assert ac["launches_per_step"] == 12 and abs(ac["share"] - 0.125) < 1e-12
+    assert abs(ac["avg_us"] - (9 * 80.0 + 3 * 90.0) / 12) < 1e-9
+    assert abs(ac["bytes"] - (9 * 200e6 + 3 * 260e6) / 12) < 1e-3
+    assert max(merged, key=lambda k: merged[k]["share"]) == "kv_ac_cell"
+    assert bench.kernel_of("k_diag_edge_v") == "kv_diag_edge" and bench.kernel_of("k_fct_cell1") == "kv_fct_cell1"
+    box = bench.host_box()
+    assert box["nproc"] >= 1 and set(box["env"]) == {"OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                                      "GPUWM_HEX_HOST_COPY_THREADS"}

@@ -93,6 +93,37 @@ def test_gemm_epilogues_match_float64(N, bn, kernel):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("bn", [128, 256])
+def test_gemm_gives_up_cleanly_when_its_wait_runs_out(bn):
+    """The persistent GEMM's bounded waits: with the MMA issuer allowed no
+    poll of its first loaded stage, every CTA gives up, reports through the
+    error word and returns (its loads and MMAs drained, tensor memory freed);
+    normal GEMMs right after it on every SM run and are correct."""
+    import time
+
+    from hexdyn import mlp
+
+    assert torch.cuda.is_available()
+    rng = np.random.default_rng(7)
+    M, N, K = 128 * 160, 2 * bn, 256  # 320 tiles: every SM's CTA takes part
+    A = om.bf16(rng.standard_normal((M, K)).astype(np.float32))
+    B = om.bf16(rng.standard_normal((N, K)).astype(np.float32) * 0.1)
+    At, Bt = _bf(A), _bf(B)
+    Cf = torch.empty(M, N, dtype=torch.float32, device="cuda")
+    t0 = time.perf_counter()
+    err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf, bn=bn, mma_wait_polls=0)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1
+    assert time.perf_counter() - t0 < 30.0
+    ref = A[:256].astype(np.float64) @ B.astype(np.float64).T
+    for _ in range(2):
+        err = mlp.gemm(At, Bt, epilogue=mlp.EPI_F32, Cf=Cf, bn=bn)
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        np.testing.assert_allclose(Cf[:256].cpu().numpy(), ref, rtol=0, atol=1e-4 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
 def test_training_gradients_match_oracle():
     from hexdyn import mlp
 

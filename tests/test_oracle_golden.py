@@ -9,7 +9,8 @@ The oracle must reproduce every output word.
 import numpy as np
 import pytest
 
-from fixtures import SIDE, STATE, VARIANTS, differing_words, golden_config, inputs, load_golden
+from fixtures import (SCALAR_VARIANTS, SIDE, STATE, VARIANTS, differing_words, digest_case, golden_config, inputs,
+                      load_digests, load_golden, mismatched_digests)
 from oracle.dycore import OracleConfig, OracleDycore, State
 
 
@@ -128,3 +129,40 @@ def test_oracle_scalar_clamp_zeroes_only_negatives():
     for k in STATE:
         if k != "scalars":
             assert differing_words(getattr(clamped, k), getattr(raw, k)) == 0, k
+
+
+@pytest.mark.parametrize("name,steps", SCALAR_VARIANTS)
+@pytest.mark.parametrize("label", ["dry", "native"])
+def test_oracle_matches_reference_scalar_counts(name, steps, label):
+    """qv + 5 condensates (the throughput workload's six scalars) and the
+    same inputs cut to 4 and 5 scalars, run by the reference with both
+    moist-coefficient semantics."""
+    fx = load_golden(name)
+    arr = inputs(fx)
+    orc = OracleDycore(arr, OracleConfig(dt=float(fx["config.dt"]), n_sub_steps=int(fx["config.n_sub_steps"]),
+                                         moist=label))
+    state, side = State(*(arr[k].copy() for k in STATE)), None
+    for step in range(1, steps + 1):
+        state, side = orc.step(state, side)
+        for k in STATE:
+            assert differing_words(getattr(state, k), fx[f"{label}.step{step}.{k}"]) == 0, (name, label, step, k)
+        for k in SIDE:
+            assert differing_words(getattr(side, k), fx[f"{label}.step{step}.side.{k}"]) == 0, (name, label, step, k)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_oracle_matches_reference_digests_at_full_size(name):
+    """2562 cells x 55 levels (two steps) and the throughput workload,
+    40962 cells x 55 levels with 6 scalars at dt 720 s (one step, about a
+    minute here): every output field of the oracle has the digest of the
+    reference's own output on the same inputs."""
+    record = load_digests(name)
+    arr, same_inputs = digest_case(record)
+    if not same_inputs:
+        pytest.skip(f"the {name} inputs built on this host differ from the recorded ones (host SIMD paths)")
+    c = record["case"]
+    orc = OracleDycore(arr, OracleConfig(dt=c["dt"], n_sub_steps=c["sub_steps"], moist=c["moist_coefficients"]))
+    state, side = State(*(np.asarray(arr[k]).copy() for k in STATE)), None
+    for step in range(1, c["steps"] + 1):
+        state, side = orc.step(state, side)
+        assert mismatched_digests(record, "native", step, state, side) == [], (name, step)

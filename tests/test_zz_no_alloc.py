@@ -1,13 +1,14 @@
 """The no-allocation step entry point against the ordinary step.
 
 ``hexdyn_step_noalloc`` exists for callers that cannot call cudaMalloc when
-they step (a stream under CUDA-graph capture, a framework whose memory pool
-must not be bypassed, members that own their state buffers but have no
-workspace): it takes caller-owned input and output buffers and keeps every
-intermediate in the library's fixed 64 MiB device array.  Its results must
-equal ``hexdyn_step`` word for word (the strict tests' tolerance) on two
-calls in a row.  The buffers below are allocated by the test itself; the
-entry point allocates nothing.
+they step (a framework whose device memory pool must not be bypassed,
+ensemble members that own their state buffers but have no workspace): it
+takes caller-owned input and output buffers and keeps every intermediate in
+the library's fixed 64 MiB device array.  Its results must equal
+``hexdyn_step`` word for word (the strict tests' tolerance) on two calls in a
+row, also right after a call on another mesh has left its words in the
+array.  The buffers below are allocated by the test itself; the entry point
+allocates nothing.
 """
 
 import ctypes as C
@@ -41,13 +42,35 @@ def _logical(drv, name, padded):
     return padded[:, :rows].t().cpu().numpy()
 
 
-@pytest.mark.parametrize("mixing", [False, True])
-def test_noalloc_step_equals_step_on_two_calls(mixing):
+def _noalloc_once(drv) -> None:
+    """One no-alloc step of ``drv``'s uploaded state into fresh buffers."""
+    import torch
+
+    atm = DeviceAtmosphere(drv)
+    f_in, f_out, keep = L.HexDynFields(), L.HexDynFields(), []
+    for k, i in L.FIELDS.items():
+        a = atm.padded(k).clone()
+        b = torch.empty_like(a)
+        keep += [a, b]
+        f_in.field[i], f_out.field[i] = a.data_ptr(), b.data_ptr()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = L.load().hexdyn_step_noalloc(drv._handle, C.byref(f_in), C.byref(f_out), stream, None)
+    assert rc == L.HEXDYN_OK, L.last_error()
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("mixing,other_mesh_first", [(False, False), (True, False), (False, True)])
+def test_noalloc_step_equals_step_on_two_calls(mixing, other_mesh_first):
     import torch
 
     if not torch.cuda.is_available():
         pytest.fail("this test needs a CUDA GPU")
     torch.cuda.set_device(0)
+    if other_mesh_first:
+        # a 642-cell, 20-level step leaves words of another layout in the array
+        other = _driver(inputs(load_golden("l3_L20")), mixing=True)
+        _noalloc_once(other)
+        other.close()
     arr = inputs(load_golden("l2_L12"))
     ref = _driver(arr, mixing)
     noa = _driver(arr, mixing)

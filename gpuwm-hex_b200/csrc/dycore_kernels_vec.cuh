@@ -1484,6 +1484,48 @@ __device__ __forceinline__ void sts4(float* p, const V4& v) {
   *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
 }
 
+// Shared memory of the column sweeps: array a of column y at
+// sm + (a * blockDim.y + y) * SP, with SP = S + 4 words per column (S is a
+// multiple of 8, so every row stays 16-byte aligned, and the odd multiple
+// of four words spreads the rows of consecutive columns over all 32 banks
+// when one thread per column sweeps them).
+#define HEX_SWEEP_PAD 4
+__device__ __forceinline__ float* sweep_col(float* sm, int a, int S, int col) {
+  return sm + ((size_t)a * blockDim.y + col) * (S + HEX_SWEEP_PAD);
+}
+__device__ __forceinline__ float* sweep_row(float* sm, int a, int S) { return sweep_col(sm, a, S, threadIdx.y); }
+
+// The sequential sweep of every column of the block.  HEX_SWEEP_BLOCK 1:
+// after a block barrier, thread t of the block sweeps column t (so one warp
+// instruction advances up to 32 columns' recurrences), then a second barrier
+// publishes the results; 0: the first lane of each column's group sweeps its
+// own column between warp barriers.  Either way each column's recurrence
+// runs in level order on one thread, so the words are the same.
+#ifndef HEX_SWEEP_BLOCK
+#define HEX_SWEEP_BLOCK 1
+#endif
+#if HEX_SWEEP_BLOCK
+#define SWEEP_BEGIN(live, k0)                                                    \
+  __syncthreads();                                                               \
+  {                                                                              \
+    const int sweep_c = threadIdx.y * blockDim.x + threadIdx.x;                  \
+    if (sweep_c < (int)blockDim.y && blockIdx.x * blockDim.y + sweep_c < g.nC) {
+#define SWEEP_END \
+  }               \
+  }               \
+  __syncthreads();
+#else
+#define SWEEP_BEGIN(live, k0)     \
+  __syncwarp();                   \
+  {                               \
+    const int sweep_c = threadIdx.y; \
+    if ((live) && (k0) == 0) {
+#define SWEEP_END \
+  }               \
+  }               \
+  __syncwarp();
+#endif
+
 // Neighbour levels across a thread's chunk: the lane below in the column
 // holds level k0-1 as its a[3], the lane above holds k0+4 as its a[0].  All
 // lanes of the warp take part; a value is used only where the one-level form
@@ -1503,9 +1545,9 @@ __global__ void HEX_VEC_BOUNDS kv_vcoef(HexGeo g, float dts2, const float* __res
   const int k0 = threadIdx.x * 4;
   const int c = blockIdx.x * blockDim.y + threadIdx.y;
   const bool live = c < g.nC && k0 < S;
-  float* s_a = sm + threadIdx.y * S * HEX_VCOEFV_SMEM_ARRAYS;
-  float* s_b = s_a + S;
-  float* s_c = s_b + S;
+  float* s_a = sweep_row(sm, 0, S);
+  float* s_b = sweep_row(sm, 1, S);
+  float* s_c = sweep_row(sm, 2, S);
   const int ii = c * S + k0;
   V4 zz = v4zero(), ex = v4zero(), th = v4zero();
   V4 wr = v4zero(), wz = v4zero(), tz = v4zero(), wt = v4zero();
@@ -1571,13 +1613,15 @@ __global__ void HEX_VEC_BOUNDS kv_vcoef(HexGeo g, float dts2, const float* __res
     sts4(s_b + k0, bv);
     sts4(s_c + k0, cv);
   }
-  __syncwarp();
-  if (live && k0 == 0) {
+  SWEEP_BEGIN(live, k0)
     // alpha overwrites b and gamma overwrites c; level 0 of both is zero
+    const float* a_col = sweep_col(sm, 0, S, sweep_c);
+    float* b_col = sweep_col(sm, 1, S, sweep_c);
+    float* c_col = sweep_col(sm, 2, S, sweep_c);
     float gam = 0.0f;
     for (int q = 0; q < L; q += 4) {
-      const V4 a4 = lds4(s_a + q);
-      V4 b4 = lds4(s_b + q), c4 = lds4(s_c + q);
+      const V4 a4 = lds4(a_col + q);
+      V4 b4 = lds4(b_col + q), c4 = lds4(c_col + q);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int kk = q + j;
@@ -1593,11 +1637,10 @@ __global__ void HEX_VEC_BOUNDS kv_vcoef(HexGeo g, float dts2, const float* __res
           c4.a[j] = gam;
         }
       }
-      sts4(s_b + q, b4);
-      sts4(s_c + q, c4);
+      sts4(b_col + q, b4);
+      sts4(c_col + q, c4);
     }
-  }
-  __syncwarp();
+  SWEEP_END
   if (live) {
     st4m(coftz + ii, tz, k0, 0, L + 1);
     st4m(cofwr + ii, wr, k0, 0, L);
@@ -1629,10 +1672,10 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
   const int k0 = threadIdx.x * 4;
   const int c = blockIdx.x * blockDim.y + threadIdx.y;
   const bool live = c < g.nC && k0 < S;
-  float* s_r = sm + threadIdx.y * S * HEX_ACV_SMEM_ARRAYS;
-  float* s_da = s_r + S;
-  float* s_al = s_da + S;
-  float* s_ga = s_al + S;
+  float* s_r = sweep_row(sm, 0, S);
+  float* s_da = sweep_row(sm, 1, S);
+  float* s_al = sweep_row(sm, 2, S);
+  float* s_ga = sweep_row(sm, 3, S);
   const int ii = c * S + k0;
   const float* ewm = g.ewm;
   const float* ewp = g.ewp;
@@ -1729,13 +1772,16 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
     }
     sts4(s_r + k0, rhs);
   }
-  __syncwarp();
   // phase 3: the dts^2 Thomas sweep (hexcore/acoustic_v841.py:236-257)
-  if (live && k0 == 0) {
-    float prev = s_r[0];
+  SWEEP_BEGIN(live, k0)
+    float* r_col = sweep_col(sm, 0, S, sweep_c);
+    const float* da_col = sweep_col(sm, 1, S, sweep_c);
+    const float* al_col = sweep_col(sm, 2, S, sweep_c);
+    const float* ga_col = sweep_col(sm, 3, S, sweep_c);
+    float prev = r_col[0];
     for (int q = 0; q < L; q += 4) {
-      V4 r = lds4(s_r + q);
-      const V4 d = lds4(s_da + q), al = lds4(s_al + q);
+      V4 r = lds4(r_col + q);
+      const V4 d = lds4(da_col + q), al = lds4(al_col + q);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int kk = q + j;
@@ -1744,12 +1790,12 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
           r.a[j] = prev;
         }
       }
-      sts4(s_r + q, r);
+      sts4(r_col + q, r);
     }
-    float next = s_r[L];
+    float next = r_col[L];
     for (int q = ((L - 1) / 4) * 4; q >= 0; q -= 4) {
-      V4 r = lds4(s_r + q);
-      const V4 ga = lds4(s_ga + q);
+      V4 r = lds4(r_col + q);
+      const V4 ga = lds4(ga_col + q);
 #pragma unroll
       for (int j = 3; j >= 0; --j) {
         const int kk = q + j;
@@ -1758,10 +1804,9 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
           r.a[j] = next;
         }
       }
-      sts4(s_r + q, r);
+      sts4(r_col + q, r);
     }
-  }
-  __syncwarp();
+  SWEEP_END
   // phase 4: implicit Rayleigh damping, ww_avg, rw_p
   V4 rwp = v4zero(), rz = v4zero();
   if (live) {

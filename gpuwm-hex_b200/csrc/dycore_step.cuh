@@ -88,13 +88,17 @@ struct Launcher {
     const int e = epb(name, tpe);
     const unsigned nb = (unsigned)((n + e - 1) / e);
     dim3 block(tpe, e), grid(fold ? nb * (unsigned)nz : nb, 1, fold ? 1 : nz);
+    run(name, grid, block, smem_per_entity * e, kernel, args...);
+  }
+  template <class K, class... A>
+  void run(const char* name, dim3 grid, dim3 block, size_t smem, K kernel, A... args) {
     HexProfEvent ev{name, nullptr, nullptr};
     if (prof) {
       cudaEventCreate(&ev.start);
       cudaEventCreate(&ev.stop);
       cudaEventRecord(ev.start, st);
     }
-    kernel<<<grid, block, smem_per_entity * e, st>>>(args...);
+    kernel<<<grid, block, smem, st>>>(args...);
     ++count;
     err = cudaGetLastError();
     if (prof) {
@@ -156,8 +160,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   HexWork& w = ctx.w;
   const int nT = ctx.n_scalars;
   const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * HEX_AC_SMEM_ARRAYS;
-  const size_t sm_vcoef_v = sizeof(float) * g.S * HEX_VCOEFV_SMEM_ARRAYS;
-  const size_t sm_ac_v = sizeof(float) * g.S * HEX_ACV_SMEM_ARRAYS;
+  const size_t sm_vcoef_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_VCOEFV_SMEM_ARRAYS;
+  const size_t sm_ac_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_ACV_SMEM_ARRAYS;
 
   if (g.moist) {
     L.lpv("k_moist_cell", g.nC, 1, kv_moist_cell, g, (const float*)in.scalars, nT, w.qtot, w.cqw);

@@ -137,17 +137,78 @@ def differing_words(a, b) -> int:
     return int(np.count_nonzero(a.view(np.uint32) != b.view(np.uint32)))
 
 
+# A read-only ``netCDF4`` for the reference's loaders, over SciPy's netCDF-3
+# reader (classic and 64-bit offset files): ``Dataset`` as a context
+# manager, ``variables`` with ``dimensions``, ``shape``, ``dtype``, ``name``
+# and indexing that returns native-endian arrays, as netCDF4-python does
+# with masking off.
+NETCDF4_SHIM = """
+import numpy as _np
+from scipy.io import netcdf_file as _nc
+
+
+class Variable:
+    def __init__(self, name, var):
+        self.name = name
+        self._var = var
+        self.dimensions = tuple(var.dimensions)
+        self.shape = tuple(var.shape)
+        self.dtype = _np.dtype(var.data.dtype).newbyteorder('=')
+        self.ndim = len(self.shape)
+
+    def __getitem__(self, index):
+        return _np.asarray(self._var.data[index]).astype(self.dtype)
+
+    def ncattrs(self):
+        return list(self._var._attributes)
+
+    def getncattr(self, name):
+        return self._var._attributes[name]
+
+    def set_auto_mask(self, flag):
+        pass
+
+    def set_auto_maskandscale(self, flag):
+        pass
+
+
+class Dataset:
+    def __init__(self, path, mode='r', **kw):
+        if mode != 'r':
+            raise RuntimeError('read-only netCDF shim')
+        self._f = _nc(str(path), 'r', mmap=False)
+        self.variables = {k: Variable(k, v) for k, v in self._f.variables.items()}
+        self.dimensions = dict(self._f.dimensions)
+
+    def ncattrs(self):
+        return list(self._f._attributes)
+
+    def getncattr(self, name):
+        return self._f._attributes[name]
+
+    def set_auto_mask(self, flag):
+        pass
+
+    def close(self):
+        self._f.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+"""
+
+
 def reference_stub_dir() -> str:
-    """A temporary directory holding a two-class ``netCDF4`` stub and a
+    """A temporary directory holding a read-only ``netCDF4`` over SciPy and a
     ``gpuwm`` stub: the reference's dycore modules import them at module
     level for file I/O and LES route checks only."""
     import tempfile
 
     d = Path(tempfile.mkdtemp(prefix="hexdyn_ref_stubs_"))
     (d / "netCDF4").mkdir()
-    (d / "netCDF4" / "__init__.py").write_text(
-        "class Dataset:\n    def __init__(self, *a, **k):\n        raise RuntimeError('no netCDF I/O')\n"
-        "class Variable:\n    pass\n")
+    (d / "netCDF4" / "__init__.py").write_text(NETCDF4_SHIM)
     (d / "gpuwm").mkdir()
     (d / "gpuwm" / "__init__.py").write_text("")
     (d / "gpuwm" / "backend.py").write_text(

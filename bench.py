@@ -434,6 +434,11 @@ def run_learned(args, plain_case) -> dict:
         "ps_rms_hpa_vs_plain": lp["ps_rms_hpa"], "theta_rel_l2_vs_plain": lp["theta_rel_l2"],
         "no_network_value": res["reduced_with_checks_no_network"]["days_per_hour"],
         "no_network_fallbacks": res["reduced_with_checks_no_network"]["fallbacks"],
+        "no_network_ps_rms_hpa_vs_plain": res["reduced_with_checks_no_network"]["ps_rms_hpa"],
+        "no_network_theta_rel_l2_vs_plain": res["reduced_with_checks_no_network"]["theta_rel_l2"],
+        "network_net_effect": ("the networks cost speed (value < no_network_value) and buy accuracy only where "
+                               "ps_rms_hpa_vs_plain < no_network_ps_rms_hpa_vs_plain; the doubled time step alone "
+                               "meets the speed target"),
         "reduced_uncorrected_first_flagged_step": res["reduced_uncorrected"]["first_flagged_step"],
         "column_net_val_loss": res["column_net"]["val_loss"],
         "column_net_val_loss_no_correction": res["column_net"]["val_loss_no_correction"],

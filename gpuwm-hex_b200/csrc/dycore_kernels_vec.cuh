@@ -5,8 +5,8 @@
 // and order exactly (one FP32 rounding per operation in the strict build);
 // the index loads, coefficient loads and address arithmetic of an entity
 // are shared by its four levels and each thread carries four independent
-// chains.  Stores are masked to the levels a field defines (levels < L, or
-// <= L for interface fields); padding words are never written.
+// chains.  Stores keep the levels a field defines (levels < L, or <= L for
+// interface fields) and write +0 into the chunk's other words (st4m).
 //
 // Thread layout: blockDim = (S/4, EPB4); x selects the chunk k0 = 4*x.
 
@@ -81,8 +81,22 @@ __device__ __forceinline__ V4 ld4rw(const float* p) {
 __device__ __forceinline__ void st4(float* p, const V4& v) {
   *reinterpret_cast<float4*>(p) = make_float4(v.a[0], v.a[1], v.a[2], v.a[3]);
 }
-// Store the lanes whose level k0+j lies in [lo, hi); other words are untouched.
+// Store the levels k0+j in [lo, hi) of a chunk; the other words of the chunk
+// (the padding levels past the field's last level, and level 0 of a field
+// defined from level 1) are written as +0.  No kernel writes anything else
+// there and every buffer starts zeroed, so those words stay +0, as they
+// would if left alone, while every lane runs the same single 128-bit store
+// (a per-word store for the chunk holding the top level would split the warp).
+#ifndef HEX_MASKED_STORE_ZERO
+#define HEX_MASKED_STORE_ZERO 1
+#endif
 __device__ __forceinline__ void st4m(float* p, const V4& v, int k0, int lo, int hi) {
+#if HEX_MASKED_STORE_ZERO
+  V4 w;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) w.a[j] = (k0 + j >= lo && k0 + j < hi) ? v.a[j] : 0.0f;
+  st4(p, w);
+#else
   if (k0 >= lo && k0 + 4 <= hi) {
     st4(p, v);
     return;
@@ -90,6 +104,7 @@ __device__ __forceinline__ void st4m(float* p, const V4& v, int k0, int lo, int 
 #pragma unroll
   for (int j = 0; j < 4; ++j)
     if (k0 + j >= lo && k0 + j < hi) p[j] = v.a[j];
+#endif
 }
 
 // Column window col[k0-4 .. k0+7] around a thread's chunk; entries outside
@@ -472,10 +487,12 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
   }
   // Perturbation-Coriolis subtraction.  With all-zero reference winds every
   // subtracted term is a signed zero, and q - (+-0) == q bit for bit unless
-  // q is itself zero or NaN, so the loop runs only when it can change a bit.
+  // q is itself zero or NaN, so the loop runs only when it can change a
+  // stored bit: the padding levels k >= L (whose u is zero) are not tested,
+  // or every warp holding a column's top chunk would run it.
   bool need = !g.winds_zero;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) need = need || !(fabsf(q.a[j]) > 0.0f);
+  for (int j = 0; j < 4; ++j) need = need || (k0 + j < g.L && !(fabsf(q.a[j]) > 0.0f));
   if (need) {
     const float fe = g.f_edge[e];
     HEX_GATHER

@@ -77,6 +77,7 @@ struct HexGeo {
   int apvm_on;
   int moist;          // 0 = dry coefficients, 1 = native (all scalars load)
   int winds_zero;     // u_init and v_init are zero at every level
+  int dss_zero;       // the implicit w damping profile dss is +0 in every word (config_xnutr = 0)
   int coc_across;     // cells_on_cell[c][s] is the cell across edges_on_cell[c][s] everywhere
   int clamp_scalars;  // negative mixing ratios set to zero at the end of the step
   // 2-D Smagorinsky mixing (hexcore/mixing_v841.py), when smag_on

@@ -17,6 +17,16 @@
 #define HEX_VEC_MIN_BLOCKS 4
 #endif
 #define HEX_VEC_BOUNDS __launch_bounds__(256, HEX_VEC_MIN_BLOCKS)
+// Third-order stencil weights A + (coef3 sign v) B selected from A + X and
+// A - X per level (1) or formed per level (0): the same words.  Measured:
+// the tracer edge values 162.6 -> 155.3 us per launch with the selection,
+// the theta/w edge values 58.5 -> 60.5 (kept per level).
+#ifndef HEX_PM_SELECT_EDGE_ADV
+#define HEX_PM_SELECT_EDGE_ADV 0
+#endif
+#ifndef HEX_PM_SELECT_TR_EDGE
+#define HEX_PM_SELECT_TR_EDGE 1
+#endif
 // Kernels measured faster at another cap: the momentum tendency (a
 // latency-bound ten-point gather) at 6 blocks (40 registers), the tracer
 // edge values (three tracers' accumulators per thread) at 2 (128), the
@@ -419,6 +429,33 @@ __global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ r
   const float* a3 = g.adv3 + (size_t)e * g.advW;
   const V4 r = ld4(ru + e * S + k0);
   const float rm = k0 > 0 ? ru[e * S + k0 - 1] : 0.0f;
+#if HEX_PM_SELECT_EDGE_ADV
+  // The stencil weight A + (coef3 sign(v)) B is A + X or A - X with
+  // X = coef3 B (a product's sign is exact, and a - b == a + (-b)): both are
+  // formed once per stencil point and each level selects by the sign bit
+  // of its velocity, the words of the per-level form.
+  bool nt[4], nw[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int k = k0 + j;
+    nt[j] = signbit(r.a[j]);
+    const float rprev = j == 0 ? rm : r.a[j - 1];
+    nw[j] = signbit(g.fzm[k] * r.a[j] + g.fzp[k] * rprev);
+  }
+  V4 at = v4zero(), aw = v4zero();
+  HEX_GATHER
+  for (int s = 0; s < n; ++s) {
+    const int cs = cells[s] * S + k0;
+    const float A = a1[s], X = g.coef3 * a3[s];
+    const float P = A + X, M = A - X;
+    const V4 th = ld4(theta + cs), wv = ld4(w + cs);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      at.a[j] = at.a[j] + (nt[j] ? M : P) * th.a[j];
+      aw.a[j] = aw.a[j] + (nw[j] ? M : P) * wv.a[j];
+    }
+  }
+#else
   float ct[4], cw[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -440,6 +477,7 @@ __global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ r
       aw.a[j] = aw.a[j] + (A + cw[j] * B) * wv.a[j];
     }
   }
+#endif
   st4m(edge_theta + e * S + k0, at, k0, 0, g.L);
   st4m(edge_w + e * S + k0, aw, k0, 1, g.L);
 }
@@ -1145,17 +1183,30 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
   const float* a1 = g.adv + (size_t)e * g.advW;
   const float* a3 = g.adv3 + (size_t)e * g.advW;
   const V4 vel = ld4(hv + e * S + k0);
+#if HEX_PM_SELECT_TR_EDGE
+  // A + (coef3 sign(vel)) B as A + X or A - X, X = coef3 B (see kv_edge_adv)
+  bool neg[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) neg[j] = signbit(vel.a[j]);
+#define HEX_TR_WEIGHTS(s_)                                   \
+  const float A = a1[s_], X = g.coef3 * a3[s_];              \
+  const float P = A + X, M = A - X;                          \
+  float w[4];                                                \
+  _Pragma("unroll") for (int j = 0; j < 4; ++j) w[j] = neg[j] ? M : P;
+#else
   float cs[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) cs[j] = g.coef3 * copysignf(1.0f, vel.a[j]);
+#define HEX_TR_WEIGHTS(s_)                                   \
+  const float A = a1[s_], B = a3[s_];                        \
+  float w[4];                                                \
+  _Pragma("unroll") for (int j = 0; j < 4; ++j) w[j] = A + cs[j] * B;
+#endif
   V4 res[TG];
   if (mono && n == 10) {
     {
       const float* qc = qg + cells[0] * S;
-      const float A = a1[0], B = a3[0];
-      float w[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) w[j] = A + cs[j] * B;
+      HEX_TR_WEIGHTS(0)
 #pragma unroll
       for (int t = 0; t < TG; ++t)
         if (t0 + t < nT) {
@@ -1167,10 +1218,7 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
     HEX_GATHER
     for (int s = 1; s < 10; ++s) {
       const float* qc = qg + cells[s] * S;
-      const float A = a1[s], B = a3[s];
-      float w[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) w[j] = A + cs[j] * B;
+      HEX_TR_WEIGHTS(s)
 #pragma unroll
       for (int t = 0; t < TG; ++t)
         if (t0 + t < nT) {
@@ -1189,13 +1237,10 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
     HEX_GATHER
     for (int s = 0; s < n; ++s) {
       const float* qc = qg + cells[s] * S;
-      const float A = a1[s], B = a3[s];
-      float w[4];
+      HEX_TR_WEIGHTS(s)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        w[j] = A + cs[j] * B;
+      for (int j = 0; j < 4; ++j)
         if (mono) w[j] = vel.a[j] * w[j];
-      }
 #pragma unroll
       for (int t = 0; t < TG; ++t)
         if (t0 + t < nT) {
@@ -1208,6 +1253,7 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
 #pragma unroll
   for (int t = 0; t < TG; ++t)
     if (t0 + t < nT) st4m(out + (size_t)(t0 + t) * g.nE * S + e * S + k0, res[t], k0, 0, g.L);
+#undef HEX_TR_WEIGHTS
 }
 
 // transport vertical flux at interface j = k0 + d (hexcore/transport.py:1389).
@@ -1673,6 +1719,11 @@ __global__ void HEX_VEC_BOUNDS kv_vcoef(HexGeo g, float dts2, const float* __res
 // expressions of k_ac_cell, four levels per thread; only the sweep's
 // operands go through shared memory.
 #define HEX_ACV_SMEM_ARRAYS 4
+// With an all-zero damping profile the acoustic cell pass skips the
+// damping's reads (1).
+#ifndef HEX_AC_DSS_ZERO_SKIP
+#define HEX_AC_DSS_ZERO_SKIP 1
+#endif
 __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float dts2, const float* __restrict__ ru_p,
                            const float* __restrict__ theta_s, const float* __restrict__ tend_rho,
                            const float* __restrict__ tend_rt, const float* __restrict__ tend_rw,
@@ -1826,25 +1877,47 @@ __global__ void HEX_VEC_BOUNDS kv_ac_cell(HexGeo g, int first, float dts, float 
   SWEEP_END
   // phase 4: implicit Rayleigh damping, ww_avg, rw_p
   V4 rwp = v4zero(), rz = v4zero();
+  const bool damping = !(HEX_AC_DSS_ZERO_SKIP && g.dss_zero);
   if (live) {
     rwp = lds4(s_r + k0);
-    rz = ld4(rho_zz + ii);
+    if (damping) rz = ld4(rho_zz + ii);
   }
   const float rz_m = from_below(rz.a[3]);
   if (live) {
-    const V4 rsv = ld4(rw_save + ii), rwv = ld4(rw + ii), dss = ld4(g.dss + ii), wv = ld4(w + ii);
+    const V4 rsv = ld4(rw_save + ii), rwv = ld4(rw + ii);
     V4 wo;
+    if (damping) {
+      const V4 dss = ld4(g.dss + ii), wv = ld4(w + ii);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = k0 + j;
-      wo.a[j] = 0.0f;
-      if (k >= 1 && k < L) {
-        const float delta = rsv.a[j] - rwv.a[j];
-        const float damp = dss.a[j];
-        const float zzi = g.fzm[k] * zz.a[j] + g.fzp[k] * (j == 0 ? zz_m : zz.a[j - 1]);
-        const float rhoi = g.fzm[k] * rz.a[j] + g.fzp[k] * (j == 0 ? rz_m : rz.a[j - 1]);
-        rwp.a[j] = (rwp.a[j] + delta - dts * damp * zzi * rhoi * wv.a[j]) / (1.0f + dts * damp) - delta;
-        wo.a[j] = wa.a[j] + ewp[k] * rwp.a[j];
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        wo.a[j] = 0.0f;
+        if (k >= 1 && k < L) {
+          const float delta = rsv.a[j] - rwv.a[j];
+          const float damp = dss.a[j];
+          const float zzi = g.fzm[k] * zz.a[j] + g.fzp[k] * (j == 0 ? zz_m : zz.a[j - 1]);
+          const float rhoi = g.fzm[k] * rz.a[j] + g.fzp[k] * (j == 0 ? rz_m : rz.a[j - 1]);
+          rwp.a[j] = (rwp.a[j] + delta - dts * damp * zzi * rhoi * wv.a[j]) / (1.0f + dts * damp) - delta;
+          wo.a[j] = wa.a[j] + ewp[k] * rwp.a[j];
+        }
+      }
+    } else {
+      // dss = +0 everywhere: the subtracted term dts (+0) zzi rhoi w is a
+      // zero with w's sign (dts, zzi and rhoi positive and finite in any
+      // state the step accepts) and the divisor is 1 + (+0) = 1, so the
+      // result is t - delta with t = rw_p + delta, except for t = -0 with
+      // w's sign bit set (then +0): w is read only there.
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        wo.a[j] = 0.0f;
+        if (k >= 1 && k < L) {
+          const float delta = rsv.a[j] - rwv.a[j];
+          float t = rwp.a[j] + delta;
+          if (__float_as_uint(t) == 0x80000000u && (__float_as_uint(w[ii + j]) & 0x80000000u)) t = 0.0f;
+          rwp.a[j] = t - delta;
+          wo.a[j] = wa.a[j] + ewp[k] * rwp.a[j];
+        }
       }
     }
     st4m(ww_avg + ii, wo, k0, 0, L + 1);

@@ -479,6 +479,12 @@ int build(HexDynHandle* h, const HexDynDesc& d, const std::vector<float>* smdiv_
   g.winds_zero = 1;
   for (int k = 0; k < L; ++k)
     if (d.u_init[k] != 0.0f || d.v_init[k] != 0.0f) g.winds_zero = 0;
+  g.dss_zero = 1;
+  for (size_t i = 0; i < (size_t)L * nC && g.dss_zero; ++i) {
+    uint32_t bits;
+    memcpy(&bits, d.dss + i, sizeof bits);
+    if (bits != 0u) g.dss_zero = 0;
+  }
 
   // schedules (hexcore/integration.py:104 RKSchedule.from_mpas): order 3
   // (dt/3, dt/2, dt; one substep of dt/3, then n/2 and n of dt/n) or order

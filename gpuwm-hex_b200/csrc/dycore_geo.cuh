@@ -102,3 +102,16 @@ struct HexGeo {
 #define HEX_FLAG_SINGULAR 2
 #define HEX_FLAG_POWF 4
 #define HEX_FLAG_TARGET 8
+
+// Physics hand-off inputs of the cell tendency kernel (all NULL when off):
+// the physics rho-theta tendency, the lagged diabatic theta, the stage's
+// density, the density tendency without physics and, at RK stage 3, the
+// modified theta dynamics rate output.
+struct HexPhysCell {
+  int on;
+  const float* rt;
+  const float* dth;
+  const float* rho;
+  const float* tend_rho_dyn;
+  float* mod_rate;
+};

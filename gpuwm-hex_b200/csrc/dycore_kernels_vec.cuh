@@ -382,7 +382,8 @@ __device__ __forceinline__ V4 mass_flux_div4(const HexGeo& g, const float* __res
 __global__ void HEX_VEC_BOUNDS kv_euler_cell(HexGeo g, const float* __restrict__ ru, const float* __restrict__ rw,
                               const float* __restrict__ pp, const float* __restrict__ rp,
                               const float* __restrict__ qtot, const float* __restrict__ cqw,
-                              float* __restrict__ tend_rho, float* __restrict__ euler_rw) {
+                              float* __restrict__ tend_rho, float* __restrict__ euler_rw,
+                              const float* __restrict__ phys_rho, float* __restrict__ tend_rho_dyn) {
   HEX_VEC_PARALLEL(g.nC)
   const int c = ent, S = g.S, L = g.L;
   const V4 hd = mass_flux_div4(g, ru, c, k0);
@@ -404,6 +405,17 @@ __global__ void HEX_VEC_BOUNDS kv_euler_cell(HexGeo g, const float* __restrict__
       out = m ? -(cq.a[j] * inner) : -inner;
     }
     er.a[j] = out;
+  }
+  if (tend_rho_dyn) {
+    // physics hand-off: the dynamics-only tendency for the modified theta
+    // rate, and the held density physics added after it
+    // (hexcore/cuda_horizontal.py:1060, density_tendency(physics_tendency=))
+    st4m(tend_rho_dyn + c * S + k0, tr, k0, 0, g.L);
+    if (phys_rho) {
+      const V4 pr = ld4(phys_rho + c * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) tr.a[j] = tr.a[j] + pr.a[j];
+    }
   }
   st4m(tend_rho + c * S + k0, tr, k0, 0, g.L);
   st4m(euler_rw + c * S + k0, er, k0, 0, g.L + 1);
@@ -500,7 +512,8 @@ template <bool RAYLEIGH>
 __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g, const float* __restrict__ u, const float* __restrict__ rw,
                           const float* __restrict__ rho, const float* __restrict__ pv_edge,
                           const float* __restrict__ ke, const float* __restrict__ hdiv,
-                          const float* __restrict__ euler_ru, float* __restrict__ tend_ru) {
+                          const float* __restrict__ euler_ru, float* __restrict__ tend_ru,
+                          const float* __restrict__ phys_ru) {
   HEX_VEC_PARALLEL(g.nE)
   const int e = ent, S = g.S;
   const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
@@ -568,6 +581,12 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
     }
     out.a[j] = res + eu.a[j];
   }
+  if (phys_ru) {
+    // (tend + saved Euler) + physics (hexcore/cuda_driver.py:4445, add_pair)
+    const V4 pu = ld4(phys_ru + e * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out.a[j] = out.a[j] + pu.a[j];
+  }
   st4m(tend_ru + e * S + k0, out, k0, 0, g.L);
 }
 
@@ -601,7 +620,8 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
                              const float* __restrict__ w, const float* __restrict__ edge_theta,
                              const float* __restrict__ edge_w, const float* __restrict__ euler_rw,
                              const float* __restrict__ tend_ru, float* __restrict__ tend_rt,
-                             float* __restrict__ tend_rw, int rk_step, const float* __restrict__ mix_theta) {
+                             float* __restrict__ tend_rw, int rk_step, const float* __restrict__ mix_theta,
+                             HexPhysCell phys) {
   HEX_VEC_PARALLEL(g.nC)
   const int c = ent, S = g.S, L = g.L;
   const int n = g.deg[c];
@@ -691,11 +711,34 @@ __global__ void HEX_VEC_BOUNDS kv_tend_cell(HexGeo g, const float* __restrict__ 
     if (k >= 1 && k < L) trw.a[j] = trw.a[j] * (g.fzm[k] * zzw(j) + g.fzp[k] * zzw(j - 1));
     if (k > L) trw.a[j] = 0.0f;
   }
+  if (phys.on) {
+    // physics hand-off (hexcore/cuda_driver.py:4459-4494): at RK stage 3 the
+    // modified theta dynamics rate (tend_rt - tend_rho theta_m) / rho of the
+    // dynamics-only tendencies, then the lagged diabatic heating rho x dth
+    const V4 rh = ld4(phys.rho + c * S + k0);
+    if (phys.mod_rate) {
+      const V4 td = ld4(phys.tend_rho_dyn + c * S + k0);
+      V4 mr;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mr.a[j] = (trt.a[j] - td.a[j] * th(j)) / rh.a[j];
+      st4m(phys.mod_rate + c * S + k0, mr, k0, 0, g.L);
+    }
+    if (phys.dth) {
+      const V4 dth = ld4(phys.dth + c * S + k0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) trt.a[j] = trt.a[j] + rh.a[j] * dth.a[j];
+    }
+  }
   if (mix_theta) {
     // hexcore/driver.py:2967: the saved horizontal theta mixing
     const V4 mt = ld4(mix_theta + c * S + k0);
 #pragma unroll
     for (int j = 0; j < 4; ++j) trt.a[j] = trt.a[j] + mt.a[j];
+  }
+  if (phys.rt) {
+    const V4 pt = ld4(phys.rt + c * S + k0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) trt.a[j] = trt.a[j] + pt.a[j];
   }
   st4m(tend_rt + c * S + k0, trt, k0, 0, g.L);
   st4m(tend_rw + c * S + k0, trw, k0, 0, g.L + 1);

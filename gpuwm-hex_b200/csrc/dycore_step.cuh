@@ -159,6 +159,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   const HexGeo& g = ctx.geo;
   HexWork& w = ctx.w;
   const int nT = ctx.n_scalars;
+  const bool hooked = ctx.stage_hook != nullptr;
+  if (hooked) ctx.phys_held_rho = 0;  // no held physics at the step's start
   const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * HEX_AC_SMEM_ARRAYS;
   const size_t sm_vcoef_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_VCOEFV_SMEM_ARRAYS;
   const size_t sm_ac_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_ACV_SMEM_ARRAYS;
@@ -194,7 +196,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
          (const float*)w.qtot, (const float*)w.cqu, w.euler_ru);
     LPS(L, g.nC, 1, euler_cell, g, (const float*)saved->rho_u, (const float*)saved->rho_w,
          (const float*)s_in->pressure_p, (const float*)s_in->rho_p, (const float*)w.qtot, (const float*)w.cqw,
-         w.tend_rho, w.euler_rw);
+         w.tend_rho, w.euler_rw, (const float*)(hooked && ctx.phys_held_rho ? ctx.phys_rho : nullptr),
+         hooked ? ctx.tend_rho_dyn : nullptr);
     L.join();
     if (g.smag_on) {
       // 2-D Smagorinsky mixing of the subcycle's start state, saved with the
@@ -222,6 +225,22 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
     for (int si = 0; si < 3; ++si) {
       const HexStage& stg = ctx.dyn[si];
       const float dts = (float)stg.acoustic_dt;
+      // physics hand-off before the stage's tendencies (the host hook runs
+      // in stream order: what it enqueues on the stream precedes the stage)
+      int phys = 0;
+      if (hooked && L.err == cudaSuccess) {
+        HexDynFields cur_fields{};
+        const float* f[HEXDYN_NUM_FIELDS] = {cur->rho, cur->rho_theta, cur->rho_u, cur->rho_w, in.scalars,
+                                             cs->theta_m, cs->exner, cs->rho_p, cs->rtheta_p, cs->pressure_p,
+                                             cs->u, cs->w};
+        for (int i = 0; i < HEXDYN_NUM_FIELDS; ++i) cur_fields.field[i] = const_cast<float*>(f[i]);
+        phys = ctx.stage_hook(ctx.stage_user, sub + 1, stg.stage, &cur_fields);
+        if (phys < 0) {
+          ctx.phys_failed = 1;
+          L.err = cudaErrorLaunchFailure;
+          break;
+        }
+      }
       // the mass-flux divergence of cur->rho_u: computed by the previous
       // stage's recovery, except for the first stage of the step
       if (sub == 0 && si == 0) LPS(L, g.nC, 1, hdiv, g, (const float*)cur->rho_u, w.hdiv);
@@ -234,7 +253,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       L.side();
       L.lpv("k_tend_u", g.nE, 1, g.rayleigh_levels ? kv_tend_u<true> : kv_tend_u<false>, g, (const float*)cs->u,
             (const float*)cur->rho_w, (const float*)cur->rho, (const float*)w.pv_edge, (const float*)w.ke,
-            (const float*)w.hdiv, saved_ru, w.tend_ru);
+            (const float*)w.hdiv, saved_ru, w.tend_ru,
+            (const float*)((phys & HEXDYN_PHYS_RHO_U) ? ctx.phys_ru : nullptr));
       if (stg.stage == 2 && ctx.order == 3) {  // hexcore/driver.py:2894
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
@@ -244,7 +264,10 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       LPS(L, g.nC, 1, tend_cell, g, (const float*)cur->rho_u, (const float*)saved->rho_u,
            (const float*)cur->rho_w, (const float*)saved->rho_w, (const float*)cs->theta_m,
            (const float*)s_in->theta_m, (const float*)cs->w, (const float*)w.edge_theta, (const float*)w.edge_w,
-           saved_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage, saved_theta);
+           saved_rw, (const float*)w.tend_ru, w.tend_rt, w.tend_rw, stg.stage, saved_theta,
+           HexPhysCell{hooked ? 1 : 0, (phys & HEXDYN_PHYS_RHO_THETA) ? ctx.phys_rt : nullptr,
+                       (phys & HEXDYN_PHYS_DIABATIC_THETA) ? ctx.phys_dth : nullptr, cur->rho,
+                       ctx.tend_rho_dyn, hooked && stg.stage == 3 ? ctx.mod_rate : nullptr});
       // acoustic substeps
       const float inv_dts = 1.0f / dts;
       const float dts2 = stg.dts2;
@@ -295,7 +318,11 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       L.join();
       cur = &o;
       cs = &so;
+      // the next subcycle's saved density tendency takes this stage's density
+      // physics when this is the subcycle's last stage
+      if (hooked && si == 2) ctx.phys_held_rho = (phys & HEXDYN_PHYS_RHO) ? 1 : 0;
     }
+    if (L.err != cudaSuccess) break;
     saved = &o;
     s_in = &so;
   }

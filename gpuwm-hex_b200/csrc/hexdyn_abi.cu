@@ -567,7 +567,8 @@ HexSide cur_side(HexDynHandle* h) { return h->ctx.parity ? h->ctx.side_out : h->
 cudaError_t enqueue_step(HexDynHandle* h, cudaStream_t st, std::vector<HexProfEvent>* prof = nullptr) {
   HexCtx& c = h->ctx;
   const int p = c.parity;
-  if (c.graph_exec[p] && !prof) return cudaGraphLaunch(c.graph_exec[p], st);
+  // a physics stage hook runs on the host between the stage launches: eager
+  if (c.graph_exec[p] && !prof && !c.stage_hook) return cudaGraphLaunch(c.graph_exec[p], st);
   const HexState& in = p ? c.out : c.in;
   const HexState& out = p ? c.in : c.out;
   const HexSide& si = p ? c.side_out : c.side_in;
@@ -669,6 +670,10 @@ int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps) {
   cudaStream_t st = (cudaStream_t)stream;
   for (int i = 0; i < nsteps; ++i) {
     cudaError_t e = enqueue_step(h, st);
+    if (h->ctx.phys_failed) {
+      h->ctx.phys_failed = 0;
+      return fail(HEXDYN_E_STATE, "the physics stage hook aborted step %d (nothing was published)", i + 1);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "step");
     h->ctx.parity ^= 1;
     h->ctx.steps_done++;
@@ -879,6 +884,8 @@ int hexdyn_step(HexDynHandle* h, void* stream, int nsteps, int* flag_out, int* c
 int hexdyn_capture_graph(HexDynHandle* h, void* stream) {
   if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
   HexCtx& c = h->ctx;
+  if (c.stage_hook)
+    return fail(HEXDYN_E_STATE, "a physics stage hook runs on the host between stages: the step stays eager");
   cudaStream_t st = (cudaStream_t)stream;
   bool own = false;
   if (!st) {
@@ -1261,6 +1268,39 @@ int hexdyn_create_ensemble(const HexDynDesc* members, int n_members, HexDynHandl
 }
 
 int hexdyn_member_count(HexDynHandle* h) { return h ? (int)h->m_c0.size() : 0; }
+
+int hexdyn_set_stage_hook(HexDynHandle* h, HexDynStageHook hook, void* user) {
+  if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
+  HexCtx& c = h->ctx;
+  if (hook && h->m_c0.size() > 1)
+    return fail(HEXDYN_E_ARG, "the physics stage hook is for single instances, not ensembles");
+  if (hook && !c.phys_ru) {
+    const HexGeo& g = c.geo;
+    const size_t CS = (size_t)g.nC * g.S, ES = (size_t)g.nE * g.S;
+    cudaError_t e;
+    if ((e = dev_alloc(c, &c.phys_ru, ES)) || (e = dev_alloc(c, &c.phys_rt, CS)) ||
+        (e = dev_alloc(c, &c.phys_rho, CS)) || (e = dev_alloc(c, &c.phys_dth, CS)) ||
+        (e = dev_alloc(c, &c.mod_rate, CS)) || (e = dev_alloc(c, &c.tend_rho_dyn, CS)))
+      return cuda_fail(e, "physics buffers");
+  }
+  c.stage_hook = hook;
+  c.stage_user = user;
+  c.phys_held_rho = 0;
+  c.phys_failed = 0;
+  return HEXDYN_OK;
+}
+
+int hexdyn_physics_buffer(HexDynHandle* h, int which, void** device_ptr) {
+  if (!h || !device_ptr) return fail(HEXDYN_E_ARG, "NULL argument");
+  HexCtx& c = h->ctx;
+  if (!c.phys_ru) return fail(HEXDYN_E_STATE, "no physics stage hook was set on this handle");
+  float* p = which == HEXDYN_PHYS_RHO_U ? c.phys_ru : which == HEXDYN_PHYS_RHO_THETA ? c.phys_rt
+           : which == HEXDYN_PHYS_RHO ? c.phys_rho : which == HEXDYN_PHYS_DIABATIC_THETA ? c.phys_dth
+           : which == HEXDYN_PHYS_MODIFIED_RATE ? c.mod_rate : nullptr;
+  if (!p) return fail(HEXDYN_E_ARG, "unknown physics buffer %d", which);
+  *device_ptr = p;
+  return HEXDYN_OK;
+}
 
 int hexdyn_set_member_state(HexDynHandle* h, int member, int field, const float* host, size_t count, void* stream) {
   return member_io(h, member, field, const_cast<float*>(host), count, stream, true);

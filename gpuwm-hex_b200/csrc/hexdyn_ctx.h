@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "../../include/hexdyn.h"
 #include "dycore_geo.cuh"
 
 struct HexState {       // prognostic state, [entity][level] padded
@@ -101,6 +102,17 @@ struct HexCtx {
   // the step graph when captured); hexdyn_step_host starts the downloads of
   // those fields on it while the scalar transport runs.
   cudaEvent_t dynamics_done = nullptr;
+  // Per-stage physics hand-off (hexdyn_set_stage_hook): the hook, its
+  // argument, the physics buffers it fills ([E][S] ru, [C][S] the others),
+  // the stage-3 modified theta rate, the density tendency without physics,
+  // and whether the last hook of the previous subcycle gave a density
+  // tendency (held into the next subcycle's saved density tendency).
+  HexDynStageHook stage_hook = nullptr;
+  void* stage_user = nullptr;
+  float *phys_ru = nullptr, *phys_rt = nullptr, *phys_rho = nullptr, *phys_dth = nullptr;
+  float *mod_rate = nullptr, *tend_rho_dyn = nullptr;
+  int phys_held_rho = 0;
+  int phys_failed = 0;  // a hook returned a negative value
   int threads_for(const char* label) const {
     if (force_threads) return force_threads;
     for (const auto& t : tuned_threads)

@@ -68,6 +68,11 @@ class HexDynDesc(C.Structure):
     ]
 
 
+# Physics stage hook (hexdyn_set_stage_hook): (user, dynamics_substep, rk_step, current fields) -> bit set
+STAGE_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(HexDynFields))
+PHYS_RHO_U, PHYS_RHO_THETA, PHYS_RHO, PHYS_DIABATIC_THETA, PHYS_MODIFIED_RATE = 1, 2, 4, 8, 16
+
+
 class HexDynBatch(C.Structure):
     """Groups of an uneven batch and their step counts (hexdyn_step_batched)."""
 
@@ -106,6 +111,8 @@ EXPORTS = {
     "hexdyn_total_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hexdyn_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
     "hexdyn_bind_state": (C.c_int, [C.c_void_p, C.POINTER(HexDynFields), C.c_void_p]),
+    "hexdyn_set_stage_hook": (C.c_int, [C.c_void_p, STAGE_HOOK, C.c_void_p]),
+    "hexdyn_physics_buffer": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

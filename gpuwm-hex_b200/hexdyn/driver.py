@@ -35,6 +35,12 @@ from .config import ConfigurationRefusal, DycoreConfig
 F32 = np.float32
 
 
+def _nullcontext():
+    import contextlib
+
+    return contextlib.nullcontext()
+
+
 def mesh_array(mesh: Any, name: str) -> np.ndarray:
     """``_mesh_array`` of the reference: attribute first, then ``mesh.arrays``."""
     try:
@@ -313,27 +319,47 @@ class HexDycoreDriver:
                           acoustic_output_callback: Any = None) -> DeviceStepResult:
         """One large step with the reference's production signature
         (hexcore/cuda_driver.py:4854, called by
-        hexcore/mpasphys/runtime_v842.py:2310).  Held physics tendencies and
-        the per-stage physics callback are outside this path and refused by
-        name before any launch.  ``physics_post_transport_callback(state=,
-        saved=, outer_state=, modified_theta_dynamics_rate=)`` is called after
-        the scalar transport, as the reference does (cuda_driver.py:5299-5305):
-        ``state`` and ``saved`` hold logical [level][entity] device views of
-        the step's result (writes land in the library's buffers and feed the
-        next step), ``outer_state`` views of the state the step started from,
-        and ``modified_theta_dynamics_rate`` is None (the reference forms it
-        only with physics tendencies).  ``acoustic_output_callback(ru_p=...,
+        hexcore/mpasphys/runtime_v842.py:2310).
+
+        ``physics_stage_callback(rk_step=, dynamics_substep=, state=, saved=,
+        diagnostics=None)`` is called before the tendencies of every RK stage
+        of every dynamics subcycle (cuda_driver.py:4393-4400) with logical
+        [level][entity] device views of the stage's state and saved
+        diagnostics; it returns an object whose ``rho_u`` [L][E],
+        ``rho_theta`` [L][C], ``rho`` [L][C] and ``diabatic_theta`` [L][C]
+        (any may be absent or None) enter the step as the reference adds
+        them: ``(tend_ru + saved Euler) + rho_u``; ``tend_rt`` + ``rho x
+        diabatic_theta``, + the saved mixing term, + ``rho_theta``; the
+        ``rho`` given at a subcycle's last stage is added to the next
+        subcycle's saved density tendency.  A callback returning None is an
+        error, as in the reference.  With a callback the step runs eagerly.
+        Held ``physics_tendencies`` belong to the reference's full-physics
+        configuration and are refused, as the reference's dry configuration
+        refuses them; ``physics_mass_loading_count`` must be the carried
+        scalar count (the moist coefficients load every carried scalar).
+
+        ``physics_post_transport_callback(state=, saved=, outer_state=,
+        modified_theta_dynamics_rate=)`` is called after the scalar transport
+        (cuda_driver.py:5299-5305): ``state`` and ``saved`` hold logical
+        device views of the step's result (writes land in the library's
+        buffers and feed the next step), ``outer_state`` views of the state
+        the step started from, and ``modified_theta_dynamics_rate`` the
+        [L][C] rate (tend_rt - tend_rho theta_m) / rho of RK stage 3 of the
+        last subcycle when a stage callback ran, else None (the reference
+        forms it only with physics tendencies).  ``acoustic_output_callback(ru_p=...,
         rw_p=...)`` receives the final acoustic words after the step (the
         reference calls it after RK stage 3 of every dynamics subcycle; its
         last call carries these values)."""
         from .config import ConfigurationRefusal
 
-        for knob, value in (("physics_tendencies", physics_tendencies),
-                            ("physics_stage_callback", physics_stage_callback),
-                            ("physics_mass_loading_count", physics_mass_loading_count)):
-            if value is not None:
-                raise ConfigurationRefusal(knob, value, "the physics coupling is not on the dry dycore step path",
-                                           f"{knob}=None")
+        if physics_tendencies is not None:
+            raise ConfigurationRefusal("held_physics_tendencies", "provided",
+                                       "a dry v8.4.1 config cannot be relabelled by supplying physics arrays",
+                                       "physics_stage_callback=... for per-stage physics, or None")
+        if physics_mass_loading_count is not None and int(physics_mass_loading_count) != self.sizes["n_scalars"]:
+            raise ConfigurationRefusal("physics_mass_loading_count", physics_mass_loading_count,
+                                       "the moist coefficients load every carried scalar on this path",
+                                       f"physics_mass_loading_count={self.sizes['n_scalars']} (or None)")
         outer = None
         if physics_post_transport_callback is not None:
             if self.config.clamp_negative_scalars:
@@ -342,14 +368,98 @@ class HexDycoreDriver:
                 raise ConfigurationRefusal("clamp_negative_scalars", True, "a post-transport callback receives "
                                            "the unclamped scalars", "clamp_negative_scalars=False")
             outer = self._views(_lib.STATE_FIELDS)  # the step reads these buffers and writes the others
-        res = self.step_device(1)
+        rate = None
+        if physics_stage_callback is None:
+            res = self.step_device(1)
+        else:
+            res = self._step_with_stage_callback(physics_stage_callback)
+            rate = self._physics_view(_lib.PHYS_MODIFIED_RATE)
         if physics_post_transport_callback is not None:
             physics_post_transport_callback(state=self._views(_lib.STATE_FIELDS),
                                             saved=self._views(_lib.SIDECAR_FIELDS), outer_state=outer,
-                                            modified_theta_dynamics_rate=None)
+                                            modified_theta_dynamics_rate=rate)
         if acoustic_output_callback is not None:
             acoustic_output_callback(**self.acoustic_words())
         return res
+
+    def _physics_view(self, which: int):
+        """Logical [L][E|C] view of a physics buffer of the library."""
+        import torch
+
+        ptr = C.c_void_p()
+        _lib.check(self._lib.hexdyn_physics_buffer(self._handle, which, C.byref(ptr)))
+        n = self.sizes["n_edges"] if which == _lib.PHYS_RHO_U else self.sizes["n_cells"]
+        t = torch.as_tensor(_CudaArray(ptr.value, (n, self.level_stride), self), device="cuda")
+        return t[:, : self.sizes["n_levels"]].t()
+
+    def _field_view(self, ptr: int, name: str):
+        import torch
+
+        n, blocks = self._entities(name)
+        rows = self._rows(name)
+        if blocks > 1:
+            t = torch.as_tensor(_CudaArray(ptr, (blocks * n, self.level_stride), self), device="cuda")
+            return t[:, :rows].reshape(blocks, n, rows).transpose(1, 2)
+        t = torch.as_tensor(_CudaArray(ptr, (n, self.level_stride), self), device="cuda")
+        return t[:, :rows].t()
+
+    def _step_with_stage_callback(self, callback) -> DeviceStepResult:
+        """One eager step with ``callback`` run before every RK stage
+        (hexdyn_set_stage_hook): the stage's fields are wrapped as views, the
+        returned tendencies copied into the library's physics buffers on the
+        step's stream."""
+        import torch
+        from types import SimpleNamespace
+
+        errors: list[BaseException] = []
+        targets = ((_lib.PHYS_RHO_U, "rho_u"), (_lib.PHYS_RHO_THETA, "rho_theta"), (_lib.PHYS_RHO, "rho"),
+                   (_lib.PHYS_DIABATIC_THETA, "diabatic_theta"))
+        stream = torch.cuda.ExternalStream(self._stream_handle().value or 0) if self._stream is not None else None
+        t0 = self.time_seconds
+
+        def hook(user, substep, rk_step, fields):
+            try:
+                f = fields.contents
+                views = {name: self._field_view(f.field[i], name) for name, i in _lib.FIELDS.items()
+                         if f.field[i] and not (name == "scalars" and self.sizes["n_scalars"] == 0)}
+                state = SimpleNamespace(**{k: views[k] for k in _lib.STATE_FIELDS if k in views}, time_seconds=t0)
+                saved = SimpleNamespace(**{k: views[k] for k in _lib.SIDECAR_FIELDS})
+                with torch.cuda.stream(stream) if stream is not None else _nullcontext():
+                    tend = callback(rk_step=int(rk_step), dynamics_substep=int(substep), state=state, saved=saved,
+                                    diagnostics=None)
+                    if tend is None:
+                        raise RuntimeError("active MPAS RK callback returned no sources")
+                    mask = 0
+                    for bit, name in targets:
+                        value = getattr(tend, name, None)
+                        if value is None:
+                            continue
+                        dst = self._physics_view(bit)
+                        src = torch.as_tensor(value, device="cuda", dtype=torch.float32)
+                        if tuple(src.shape) != tuple(dst.shape):
+                            raise ValueError(f"physics {name} shape {tuple(src.shape)} != {tuple(dst.shape)}")
+                        dst.copy_(src)
+                        mask |= bit
+                return mask
+            except BaseException as exc:  # noqa: BLE001 - reported after the step
+                errors.append(exc)
+                return -1
+
+        cb = _lib.STAGE_HOOK(hook)
+        _lib.check(self._lib.hexdyn_set_stage_hook(self._handle, cb, None))
+        try:
+            flag = C.c_int(0)
+            done = C.c_int(0)
+            rc = self._lib.hexdyn_step(self._handle, self._stream_handle(), 1, C.byref(flag), C.byref(done))
+        finally:
+            self._lib.hexdyn_set_stage_hook(self._handle, _lib.STAGE_HOOK(), None)
+        if errors:
+            raise errors[0]
+        if rc == _lib.HEXDYN_E_NUMERIC:
+            raise FloatingPointError(_lib.last_error())
+        _lib.check(rc)
+        self.time_seconds += self.config.config_dt
+        return DeviceStepResult(DeviceAtmosphere(self), self.receipt(1, flag.value))
 
     def _views(self, names) -> Any:
         """Logical device views of the current buffers of ``names`` (with

@@ -242,6 +242,35 @@ typedef struct HexDynFields {
   float* field[HEXDYN_NUM_FIELDS];
 } HexDynFields;
 
+/* Per-stage physics hand-off: `physics_stage_callback` of the reference's
+ * `_step_device_v841` (hexcore/cuda_driver.py:4393-4400, called by
+ * hexcore/mpasphys/runtime_v842.py:2310).  With a hook set, every large
+ * step runs eagerly (no graph) and calls the hook on the host before the
+ * tendencies of each RK stage of each dynamics subcycle, in stream order,
+ * with `current` holding device pointers (padded layout) of the stage's
+ * state and saved diagnostics.  The hook fills the physics buffers of
+ * hexdyn_physics_buffer on the step's stream and returns a bit set of what
+ * it gave (HEXDYN_PHYS_*), or a negative value to abort the step (the step
+ * returns HEXDYN_E_STATE).  The tendencies enter as the reference adds them:
+ * tend_ru = (tend_ru + saved Euler u term) + rho_u; tend_rt gains, after its
+ * stage-3 modified-rate snapshot, rho x diabatic_theta, the saved mixing
+ * term, then rho_theta; the density tendency that the hook gave at the last
+ * stage of a subcycle is added to the next subcycle's saved density
+ * tendency.  At RK stage 3 of every subcycle the step stores the modified
+ * theta dynamics rate (tend_rt - tend_rho theta_m) / rho, before any
+ * physics term, in buffer HEXDYN_PHYS_MODIFIED_RATE.  Single instances only;
+ * `hook` NULL removes it. */
+#define HEXDYN_PHYS_RHO_U 1
+#define HEXDYN_PHYS_RHO_THETA 2
+#define HEXDYN_PHYS_RHO 4
+#define HEXDYN_PHYS_DIABATIC_THETA 8
+#define HEXDYN_PHYS_MODIFIED_RATE 16
+typedef int (*HexDynStageHook)(void* user, int dynamics_substep, int rk_step, const struct HexDynFields* current);
+int hexdyn_set_stage_hook(HexDynHandle* h, HexDynStageHook hook, void* user);
+/* Device pointer of a physics buffer ([E][S] for HEXDYN_PHYS_RHO_U, [C][S]
+ * otherwise; padded layout, zeroed when the hook is set). */
+int hexdyn_physics_buffer(HexDynHandle* h, int which, void** device_ptr);
+
 /* Bind caller-owned device buffers (padded layout, 16-byte aligned, every
  * field; replaces the reference's DeviceAtmosphere handed to the driver,
  * hexcore/cuda_driver.py:5419) as the current state

@@ -76,6 +76,10 @@ class OracleConfig:
     smagorinsky: Any = None     # oracle.mixing.SmagorinskyConfig: 2-D Smagorinsky mixing on
     rayleigh: Any = None        # (levels, days): Rayleigh damping of u over the top levels
     clamp_negative_scalars: bool = False  # cuda_driver.py:5311 end-of-step clamp
+    # Per-stage physics hand-off (hexcore/cuda_driver.py:4393-4400):
+    # callable(rk_step=, dynamics_substep=, state=State, saved=Sidecar) ->
+    # object with rho_u / rho_theta / rho / diabatic_theta (or None each)
+    physics_stage: Any = None
 
 
 def schedule(dt: float, n_sub: int, splits: int, order: int = 3):
@@ -665,7 +669,7 @@ class OracleDycore:
             theta[:, g.c0] + theta[:, g.c1])
 
     # ----------------------------------------------------------- subcycle
-    def subcycle(self, state: State, T1: Sidecar, diag: Diag, moist, record=None):
+    def subcycle(self, state: State, T1: Sidecar, diag: Diag, moist, record=None, substep: int = 1):
         g = self.g
         cfg = self.cfg
         L = g.nlev
@@ -681,6 +685,12 @@ class OracleDycore:
         cur_u, cur_w = T1.normal_velocity.copy(), T1.vertical_velocity.copy()
         cached_v = diag.v
         euler_ru, tend_rho, euler_rw = self.euler_terms(saved, T1, qtot, cqw, cqu)
+        # the density physics of the previous subcycle's last stage joins the
+        # saved density tendency (hexcore/cuda_driver.py:4275-4305,
+        # density_tendency(physics_tendency=) adds it last)
+        tend_rho_dyn = tend_rho
+        if cfg.physics_stage is not None and getattr(self, "_held_rho", None) is not None:
+            tend_rho = tend_rho + self._held_rho
         mix_theta = None
         if self.smag is not None:
             # driver.py:2826-2880: the mixing of the subcycle's start state,
@@ -690,6 +700,13 @@ class OracleDycore:
                 diag.extra["divergence"], diag.extra["vorticity"], euler_ru, euler_rw)
         flux_u = flux_w = None
         for stage, large_dt, dts, n_ac in stages:
+            phys = None
+            if cfg.physics_stage is not None:
+                phys = cfg.physics_stage(
+                    rk_step=stage, dynamics_substep=substep, state=cur,
+                    saved=Sidecar(cur_theta, cur_exner, cur_rp, cur_rtp, cur_pp, cur_u, cur_w))
+                if phys is None:
+                    raise RuntimeError("active MPAS RK callback returned no sources")
             if stage == 2 and cfg.order == 3:  # driver.py:2894
                 co = self.vertical_coefficients(dts, exner_s, cur_theta, cur_rtp, cqw, qtot)
             rho_edge = HALF * (cur.rho[:, g.c0] + cur.rho[:, g.c1])
@@ -704,9 +721,20 @@ class OracleDycore:
                 for k in range(L - levels, L):
                     tend_ru[k] = tend_ru[k] - (rho_edge[k] * cur_u[k]) * (F32(k - (L - levels) + 1) * inv)
             tend_ru = tend_ru + euler_ru
+            if phys is not None and getattr(phys, "rho_u", None) is not None:
+                tend_ru = tend_ru + phys.rho_u  # cuda_driver.py:4445 add_pair
             tend_rt = self.rho_theta_tendency(cur, saved, cur_theta, theta_s, stage)
+            if phys is not None:
+                if stage == 3:
+                    # cuda_driver.py:4459-4475 modified_theta_dynamics_rate
+                    self.modified_rate = (tend_rt - tend_rho_dyn * cur_theta) / cur.rho
+                dth = getattr(phys, "diabatic_theta", None)
+                if dth is not None:
+                    tend_rt = tend_rt + cur.rho * dth  # add_lagged_diabatic_theta
             if mix_theta is not None:
                 tend_rt = tend_rt + mix_theta  # driver.py:2967
+            if phys is not None and getattr(phys, "rho_theta", None) is not None:
+                tend_rt = tend_rt + phys.rho_theta  # cuda_driver.py:4489-4494
             tend_rw = self.w_tendency(cur, cur_w)
             tend_rw = tend_rw + euler_rw
             tend_om = self.omega(tend_rw, tend_ru)
@@ -751,6 +779,8 @@ class OracleDycore:
             cur_w = self.vertical_velocity(cur.rho, cur.rho_u, cur.rho_w)
             diag = self.diagnostics(cur.rho, cur_u, stage, cached_v)
             cached_v = diag.v
+            if phys is not None and stage == stages[-1][0]:
+                self._held_rho = getattr(phys, "rho", None)
         side = Sidecar(cur_theta.copy(), cur_exner.copy(), cur_rp.copy(), cur_rtp.copy(),
                        cur_pp.copy(), cur_u.copy(), cur_w.copy())
         return cur, side, diag, flux_u, flux_w
@@ -901,8 +931,10 @@ class OracleDycore:
         diag = self.diagnostics(outer.rho, T0.normal_velocity, 3, None)
         cur, carried = outer, T0
         fu_sum = fw_sum = None
-        for _ in range(cfg.split_steps):
-            cur, carried, diag, fu, fw = self.subcycle(cur, carried, diag, moist, record)
+        self._held_rho = None
+        self.modified_rate = None
+        for sub in range(cfg.split_steps):
+            cur, carried, diag, fu, fw = self.subcycle(cur, carried, diag, moist, record, substep=sub + 1)
             fu_sum = fu.copy() if fu_sum is None else fu + fu_sum
             fw_sum = fw.copy() if fw_sum is None else fw + fw_sum
         inv = ONE / F32(cfg.split_steps)

@@ -340,22 +340,24 @@ def test_validation_flag_raises_on_bad_state():
 
 
 def test_acoustic_words_and_reference_step_signature():
-    """_step_device_v841 (the reference's production entry) refuses the
-    held-tendency physics hand-offs by name and hands acoustic_output_callback the final
-    acoustic words, equal to the oracle's ru_p and rw_p after the last
-    substep of RK stage 3 of the last subcycle."""
+    """_step_device_v841 (the reference's production entry) refuses held
+    physics tendencies and a mass-loading count other than the carried
+    scalars by name, and hands acoustic_output_callback the final acoustic
+    words, equal to the oracle's ru_p and rw_p after the last substep of RK
+    stage 3 of the last subcycle (the per-stage physics callback:
+    tests/test_physics_hook.py)."""
     from hexdyn.config import ConfigurationRefusal
     from oracle.dycore import OracleConfig, OracleDycore, State
 
     fx = load_golden("l2_L12")
     arr = inputs(fx)
     drv = make_driver(arr, float(fx["config.dt"]), int(fx["config.n_sub_steps"]), "dry", graph=True)
-    for kw in ("physics_stage_callback", "physics_mass_loading_count"):
-        with pytest.raises(ConfigurationRefusal) as err:
-            drv._step_device_v841(**{kw: 1})
-        assert err.value.knob == kw
-    with pytest.raises(ConfigurationRefusal):
+    with pytest.raises(ConfigurationRefusal) as err:
+        drv._step_device_v841(physics_mass_loading_count=arr["scalars"].shape[0] + 1)
+    assert err.value.knob == "physics_mass_loading_count"
+    with pytest.raises(ConfigurationRefusal) as err:
         drv._step_device_v841(object())
+    assert err.value.knob == "held_physics_tendencies"
     got = {}
 
     def keep(ru_p, rw_p):

@@ -70,10 +70,13 @@ def parse() -> argparse.Namespace:
 
 
 # ------------------------------------------------------------- byte model
-def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 6, advW: int = 10) -> int:
+def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 6, advW: int = 10,
+                 damping: bool = False) -> int:
     """Algorithmic bytes of one launch: each distinct array read or written,
     times the extent it touches (L levels or L+1 interfaces per entity), 4 B,
-    counted once; connectivity/coefficient tables counted once."""
+    counted once; connectivity/coefficient tables counted once.  ``damping``:
+    the implicit w damping profile is not zero (config_xnutr > 0), so the
+    acoustic cell pass also reads dss, rho_zz and w."""
     cl, ci, el, vl = C * L, C * (L + 1), E * L, V * L
     tcl, tel = T * C * L, T * E * L
     conn_c = C * maxE * 3 + C * 2          # eoc, csign (+ coc/voc) and deg, inv_area
@@ -98,8 +101,9 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_ac_edge_first": 3 * el,                                 # tend_ru in; ru_p, ru_avg out
         "k_ac_edge": 7 * el + 6 * cl + conn_e,                     # damping of n-1 + update n
         "k_ac_edge_damp": 2 * el + 3 * cl + conn_e,                # damping only
-        "k_ac_cell_first": el + 12 * cl + 7 * ci + conn_c,        # old perturbations are zero
-        "k_ac_cell": el + 16 * cl + 9 * ci + conn_c,
+        # (+ dss, rho_zz, w when the damping profile is not zero)
+        "k_ac_cell_first": el + 10 * cl + 6 * ci + conn_c + (2 * cl + ci if damping else 0),  # old perts zero
+        "k_ac_cell": el + 14 * cl + 8 * ci + conn_c + (2 * cl + ci if damping else 0),
         "k_recover_edge": 7 * el + 3 * cl + conn_e,
         "k_recover_cell": el + 16 * cl + 7 * ci + zb + conn_c,       # + the next stage's hdiv
         "k_tr_edge": (tcl + tel) + el + adv,
@@ -543,12 +547,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         try:
-            # ncu DRAM bytes per launch, per label; a kernel's is the
-            # launch-weighted mean over its labels (None unless all were captured)
+            # ncu DRAM bytes per launch of each kernel function (the mean
+            # over its launches of one step)
             known = json.loads(traffic_file.read_text())
-            if all(lb in known for lb in dk["labels"]):
-                traffic = sum(known[lb] * kernels[lb]["launches_per_step"] for lb in dk["labels"]) / \
-                    dk["launches_per_step"]
+            traffic = known.get(dominant)
         except Exception:  # noqa: BLE001
             traffic = None
     step_bytes = sum(kernel_bytes(k, C, E, V, L, T) * kernels[k]["launches_per_step"] for k in kernels)

@@ -1,3 +1,5 @@
+#include <initializer_list>
+#include <utility>
 // Step orchestration: hexcore/driver.py:3314 DryDycoreDriver.step with the
 // v8.4.1 subcycle of hexcore/driver.py:2710, as a fixed sequence of kernel
 // launches on one stream (capturable into one CUDA graph).
@@ -161,6 +163,27 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   const int nT = ctx.n_scalars;
   const bool hooked = ctx.stage_hook != nullptr;
   if (hooked) ctx.phys_held_rho = 0;  // no held physics at the step's start
+  // halo exchange at a named point (a partitioned instance): the buffers and
+  // their kinds; a failing hook stops the launches
+  auto exchange = [&](int point, std::initializer_list<std::pair<const float*, int>> list) {
+    if (!ctx.exchange_hook || L.err != cudaSuccess) return;
+    float* bufs[24];
+    int kinds[24];
+    int n = 0;
+    for (const auto& b : list)
+      if (b.first && n < 24) {
+        bufs[n] = const_cast<float*>(b.first);
+        kinds[n++] = b.second;
+      }
+    if (ctx.exchange_hook(ctx.exchange_user, point, n, bufs, kinds) < 0) {
+      ctx.phys_failed = 1;
+      L.err = cudaErrorLaunchFailure;
+    }
+  };
+  const int KC = HEXDYN_KIND_CELL, KE = HEXDYN_KIND_EDGE, KT = HEXDYN_KIND_TRACER;
+  exchange(HEXDYN_XCH_STATE, {{in.rho, KC}, {in.rho_theta, KC}, {in.rho_u, KE}, {in.rho_w, KC}, {in.scalars, KT},
+                              {side_in.theta_m, KC}, {side_in.exner, KC}, {side_in.rho_p, KC}, {side_in.rtheta_p, KC},
+                              {side_in.pressure_p, KC}, {side_in.u, KE}, {side_in.w, KC}});
   const size_t sm_vcoef = sizeof(float) * g.S * 7, sm_ac = sizeof(float) * g.S * HEX_AC_SMEM_ARRAYS;
   const size_t sm_vcoef_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_VCOEFV_SMEM_ARRAYS;
   const size_t sm_ac_v = sizeof(float) * (g.S + HEX_SWEEP_PAD) * HEX_ACV_SMEM_ARRAYS;
@@ -171,6 +194,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
   }
   // initial solve diagnostics with v reconstructed (rk_step=3)
   diagnostics(L, side_in.u, 1);
+  exchange(HEXDYN_XCH_DIAG, {{w.pv_edge, KE}, {w.ke, KC}, {w.v, KE}});
 
   const HexState* saved = &in;
   const HexSide* s_in = &side_in;
@@ -292,6 +316,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
              (const float*)w.cofwt, (const float*)w.a_tri, (const float*)w.alpha_tri, (const float*)w.gamma_tri,
              (const float*)cur->rho, (const float*)cs->w, (const float*)cur->rho_w, (const float*)saved->rho_w,
              old_rt, new_rt, w.rho_pp, w.rw_p, w.ww_avg);
+        exchange(HEXDYN_XCH_ACOUSTIC, {{w.rho_pp, KC}, {new_rt, KC}, {w.rw_p, KC}, {w.ww_avg, KC}, {w.ru_p, KE},
+                                       {w.ru_avg, KE}});
       }
       {
         const int n = stg.acoustic_steps;
@@ -316,6 +342,9 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       L.side();
       diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
       L.join();
+      exchange(HEXDYN_XCH_STATE, {{o.rho, KC}, {o.rho_theta, KC}, {o.rho_u, KE}, {o.rho_w, KC}, {so.theta_m, KC},
+                                  {so.exner, KC}, {so.rho_p, KC}, {so.rtheta_p, KC}, {so.pressure_p, KC},
+                                  {so.u, KE}, {so.w, KC}, {w.pv_edge, KE}, {w.ke, KC}, {w.v, KE}, {w.hdiv, KC}});
       cur = &o;
       cs = &so;
       // the next subcycle's saved density tendency takes this stage's density
@@ -344,6 +373,10 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       const HexStage& stg = ctx.scal[si];
       const float step = (float)stg.large_dt;
       float* q_next = si == 2 ? out.scalars : w.q_stage[si];
+      if (si == 0)
+        exchange(HEXDYN_XCH_SCALARS, {{q_prev, KT}, {w.flux_u, KE}, {w.flux_w, KC}});
+      else
+        exchange(HEXDYN_XCH_SCALARS, {{q_prev, KT}});
       if (si < 2 || !ctx.monotonic) {
         // hexcore/transport.py:1749-1755 time-interpolation weight of rho_new
         const float wn = si == 0 ? (ctx.order == 3 ? (float)(1.0 / 3.0) : 0.5f) : (si == 1 ? 0.5f : 1.0f);
@@ -359,6 +392,7 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         L.lpvt("k_fct_cell1", g.nC, nT, g.coc_across ? kv_fct_cell1<true> : kv_fct_cell1<false>, g, nT, step,
              (const float*)in.scalars, q_prev, (const float*)in.rho, (const float*)w.flux_u, (const float*)w.flux_w, (const float*)w.edge_q, (const float*)w.target,
              w.scale_in, w.scale_out, w.mass, w.vres);
+        exchange(HEXDYN_XCH_FCT, {{w.scale_in, KT}, {w.scale_out, KT}});
         LPST(L, g.nE, nT, fct_edge, g, step, (const float*)in.scalars, (const float*)w.flux_u,
              (const float*)w.edge_q, (const float*)w.scale_in, (const float*)w.scale_out, w.hres_lim);
         LPST(L, g.nC, nT, fct_cell2, g, (const float*)w.vres, (const float*)w.scale_in, (const float*)w.scale_out, (const float*)w.mass, (const float*)w.hres_lim,

@@ -568,7 +568,7 @@ cudaError_t enqueue_step(HexDynHandle* h, cudaStream_t st, std::vector<HexProfEv
   HexCtx& c = h->ctx;
   const int p = c.parity;
   // a physics stage hook runs on the host between the stage launches: eager
-  if (c.graph_exec[p] && !prof && !c.stage_hook) return cudaGraphLaunch(c.graph_exec[p], st);
+  if (c.graph_exec[p] && !prof && !c.stage_hook && !c.exchange_hook) return cudaGraphLaunch(c.graph_exec[p], st);
   const HexState& in = p ? c.out : c.in;
   const HexState& out = p ? c.in : c.out;
   const HexSide& si = p ? c.side_out : c.side_in;
@@ -672,7 +672,7 @@ int hexdyn_step_async(HexDynHandle* h, void* stream, int nsteps) {
     cudaError_t e = enqueue_step(h, st);
     if (h->ctx.phys_failed) {
       h->ctx.phys_failed = 0;
-      return fail(HEXDYN_E_STATE, "the physics stage hook aborted step %d (nothing was published)", i + 1);
+      return fail(HEXDYN_E_STATE, "a physics or halo exchange hook aborted step %d (nothing was published)", i + 1);
     }
     if (e != cudaSuccess) return cuda_fail(e, "step");
     h->ctx.parity ^= 1;
@@ -884,8 +884,9 @@ int hexdyn_step(HexDynHandle* h, void* stream, int nsteps, int* flag_out, int* c
 int hexdyn_capture_graph(HexDynHandle* h, void* stream) {
   if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
   HexCtx& c = h->ctx;
-  if (c.stage_hook)
-    return fail(HEXDYN_E_STATE, "a physics stage hook runs on the host between stages: the step stays eager");
+  if (c.stage_hook || c.exchange_hook)
+    return fail(HEXDYN_E_STATE, "a physics or halo exchange hook runs on the host between stages: the step stays "
+                "eager");
   cudaStream_t st = (cudaStream_t)stream;
   bool own = false;
   if (!st) {
@@ -1287,6 +1288,16 @@ int hexdyn_set_stage_hook(HexDynHandle* h, HexDynStageHook hook, void* user) {
   c.stage_user = user;
   c.phys_held_rho = 0;
   c.phys_failed = 0;
+  return HEXDYN_OK;
+}
+
+int hexdyn_set_exchange_hook(HexDynHandle* h, HexDynExchangeHook hook, void* user) {
+  if (!h) return fail(HEXDYN_E_ARG, "NULL handle");
+  if (hook && h->m_c0.size() > 1)
+    return fail(HEXDYN_E_ARG, "the halo exchange hook is for single instances, not ensembles");
+  h->ctx.exchange_hook = hook;
+  h->ctx.exchange_user = user;
+  h->ctx.phys_failed = 0;
   return HEXDYN_OK;
 }
 

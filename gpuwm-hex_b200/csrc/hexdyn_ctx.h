@@ -113,6 +113,9 @@ struct HexCtx {
   float *mod_rate = nullptr, *tend_rho_dyn = nullptr;
   int phys_held_rho = 0;
   int phys_failed = 0;  // a hook returned a negative value
+  // Halo exchange hook of a partitioned instance (hexdyn_set_exchange_hook)
+  HexDynExchangeHook exchange_hook = nullptr;
+  void* exchange_user = nullptr;
   int threads_for(const char* label) const {
     if (force_threads) return force_threads;
     for (const auto& t : tuned_threads)

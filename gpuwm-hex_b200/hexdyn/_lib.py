@@ -71,6 +71,10 @@ class HexDynDesc(C.Structure):
 # Physics stage hook (hexdyn_set_stage_hook): (user, dynamics_substep, rk_step, current fields) -> bit set
 STAGE_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(HexDynFields))
 PHYS_RHO_U, PHYS_RHO_THETA, PHYS_RHO, PHYS_DIABATIC_THETA, PHYS_MODIFIED_RATE = 1, 2, 4, 8, 16
+# Halo exchange hook (hexdyn_set_exchange_hook): (user, point, nbufs, device buffers, kinds) -> 0 / negative
+EXCHANGE_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int))
+XCH_STATE, XCH_DIAG, XCH_ACOUSTIC, XCH_SCALARS, XCH_FCT = 1, 2, 3, 4, 5
+KIND_CELL, KIND_EDGE, KIND_TRACER = 0, 1, 2
 
 
 class HexDynBatch(C.Structure):
@@ -113,6 +117,7 @@ EXPORTS = {
     "hexdyn_bind_state": (C.c_int, [C.c_void_p, C.POINTER(HexDynFields), C.c_void_p]),
     "hexdyn_set_stage_hook": (C.c_int, [C.c_void_p, STAGE_HOOK, C.c_void_p]),
     "hexdyn_physics_buffer": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "hexdyn_set_exchange_hook": (C.c_int, [C.c_void_p, EXCHANGE_HOOK, C.c_void_p]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -587,3 +587,21 @@ def case_arrays(case: DycoreCase) -> dict[str, Any]:
     out["coef_3rd_order"] = case.coef_3rd_order
     out["scalar_names"] = np.array(case.scalar_names)
     return out
+
+
+def arrays_case(arr: dict[str, Any]) -> DycoreCase:
+    """The case of a flat array dict (inverse of ``case_arrays``)."""
+    mesh = VoronoiMesh(arrays={k[5:]: v for k, v in arr.items() if k.startswith("mesh.")})
+    vfields = {k[9:]: v for k, v in arr.items() if k.startswith("vertical.")}
+    for k in ("cf1", "cf2", "cf3"):
+        vfields[k] = float(vfields[k])
+    vfields["first_height_level"] = int(vfields["first_height_level"])
+    names = arr.get("scalar_names")
+    names = tuple(str(n) for n in np.asarray(names).reshape(-1)) if names is not None else \
+        tuple(f"q{i}" for i in range(np.asarray(arr["scalars"]).shape[0]))
+    return DycoreCase(mesh=mesh, vertical=VerticalGridData(**vfields), scalar_names=names,
+                      coef_3rd_order=float(arr.get("coef_3rd_order", 0.25)),
+                      **{k: arr[k] for k in ("zb_cell", "zb3_cell", "rho_base", "rho_theta_base", "pressure_base",
+                                             "exner_base", "rho", "rho_theta", "rho_u", "rho_w", "scalars",
+                                             "adv_coefs", "adv_coefs_3rd", "n_adv_cells_for_edge",
+                                             "adv_cells_for_edge", "u_init", "v_init")})

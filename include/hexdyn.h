@@ -271,6 +271,40 @@ int hexdyn_set_stage_hook(HexDynHandle* h, HexDynStageHook hook, void* user);
  * otherwise; padded layout, zeroed when the hook is set). */
 int hexdyn_physics_buffer(HexDynHandle* h, int which, void** device_ptr);
 
+/* Halo exchange hook of a partitioned instance (one rank's local mesh:
+ * owned entities first, halo entities last; hexdyn.partition builds the
+ * meshes and the plan).  With a hook set, every step runs eagerly and calls
+ * it on the host, in stream order and with both streams joined, at the
+ * points where owner values must reach the halo -- the reference's rounds
+ * (hexcore/partition_executor_v841.py:35-50):
+ *   HEXDYN_XCH_STATE     the step's start (state, saved diagnostics and
+ *                        scalars) and the end of every RK stage after the
+ *                        recovery and the solve diagnostics (state, saved
+ *                        diagnostics, pv_edge, ke, v and the mass-flux
+ *                        divergence);
+ *   HEXDYN_XCH_DIAG      after the step's initial solve diagnostics (pv_edge,
+ *                        ke, v);
+ *   HEXDYN_XCH_ACOUSTIC  after every acoustic cell pass (rho_pp, rtheta_pp,
+ *                        rw_p, ww_avg, ru_p, ru_avg);
+ *   HEXDYN_XCH_SCALARS   at the entry of every transport stage (the stage's
+ *                        input scalars; at the first also the split mass
+ *                        fluxes);
+ *   HEXDYN_XCH_FCT       after the monotonic limiter's scale factors.
+ * `bufs[i]` is a device buffer in the padded layout of kind `kinds[i]`
+ * (HEXDYN_KIND_*); the hook overwrites its halo rows with the owners'
+ * values on the step's stream and returns 0, or a negative value to abort
+ * the step.  Single instances only; `hook` NULL removes it. */
+#define HEXDYN_XCH_STATE 1
+#define HEXDYN_XCH_DIAG 2
+#define HEXDYN_XCH_ACOUSTIC 3
+#define HEXDYN_XCH_SCALARS 4
+#define HEXDYN_XCH_FCT 5
+#define HEXDYN_KIND_CELL 0    /* [nCells][S] */
+#define HEXDYN_KIND_EDGE 1    /* [nEdges][S] */
+#define HEXDYN_KIND_TRACER 2  /* [n_scalars][nCells][S] */
+typedef int (*HexDynExchangeHook)(void* user, int point, int nbufs, float* const* bufs, const int* kinds);
+int hexdyn_set_exchange_hook(HexDynHandle* h, HexDynExchangeHook hook, void* user);
+
 /* Bind caller-owned device buffers (padded layout, 16-byte aligned, every
  * field; replaces the reference's DeviceAtmosphere handed to the driver,
  * hexcore/cuda_driver.py:5419) as the current state

@@ -1,0 +1,134 @@
+"""Partitioned single instance on the device: every rank's owned region
+equals the single instance, word for word (the reference's partition
+invariance, ``hexcore/partition_executor_v841.py``: owned-region union
+byte-compared with the single-GPU run at every step boundary).
+
+The ranks run in one process on one GPU (``hexdyn.partition.PartitionedDycore``:
+a thread and a stream per rank, halo exchanges as device copies ordered by
+events); the layouts, plans and exchange points are those a rank per GPU
+uses (``RankDycore``).  The workload is 2562 cells x 55 levels renumbered
+along a Hilbert curve, qv + 5 condensates (the limiter's exchange runs),
+dt 720 s, two steps.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import hexdyn
+from fixtures import differing_words
+from hexdyn import _lib, partition, reorder
+from hexdyn.case import arrays_case, build_case, case_arrays
+from hexdyn.config import DycoreConfig
+from hexdyn.mesh import build_mesh
+
+pytestmark = pytest.mark.gpu
+
+SMAG = dict(config_horiz_mixing="2d_smagorinsky", config_smagorinsky_coef=0.125, config_visc4_2dsmag=0.05)
+
+
+@pytest.fixture(scope="module")
+def arrays():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("these tests need a CUDA GPU")
+    torch.cuda.set_device(0)
+    arr = case_arrays(build_case(build_mesh(4, lloyd=20, seed=0), n_levels=55, seed=0, n_condensates=5))
+    return reorder.apply(arr, reorder.hilbert_order(arr))
+
+
+def _config(mixing):
+    return DycoreConfig(config_dt=720.0, config_number_of_sub_steps=2, moist_coefficients="native",
+                        **(SMAG if mixing else {}))
+
+
+def _single(arr, cfg, steps):
+    drv = hexdyn.from_case(arrays_case(arr), cfg)
+    out = []
+    for _ in range(steps):
+        drv.step_device(1)
+        st, sd = drv.get_state()
+        out.append(({k: getattr(st, k) for k in _lib.STATE_FIELDS}, {k: getattr(sd, k) for k in _lib.SIDECAR_FIELDS}))
+    drv.close()
+    return out
+
+
+def _differing(got, want) -> dict:
+    bad = {}
+    for part in (0, 1):
+        for k, v in want[part].items():
+            n = differing_words(got[part][k], v)
+            if n:
+                bad[k] = n
+    return bad
+
+
+# per step: the start and the end of each of 3 subcycles x 3 RK stages; the
+# initial diagnostics; one acoustic cell pass per substep (1, 1, 2 substeps
+# at 2 substeps per stage); 3 transport stages; the limiter once
+EXCHANGES_PER_STEP = {_lib.XCH_STATE: 10, _lib.XCH_DIAG: 1, _lib.XCH_ACOUSTIC: 12, _lib.XCH_SCALARS: 3,
+                      _lib.XCH_FCT: 1}
+
+
+@pytest.mark.parametrize("n_parts,mixing", [(2, False), (4, False), (3, True)])
+def test_partitioned_steps_are_the_single_instance(arrays, n_parts, mixing):
+    cfg = _config(mixing)
+    want = _single(arrays, cfg, 2)
+    part = partition.PartitionedDycore(arrays, cfg, n_parts)
+    assert all(lay.l2g["cell"].size > lay.n_owned["cell"] for lay in part.layouts)
+    for step in range(2):
+        part.step(1)
+        assert _differing(part.get_state(), want[step]) == {}, (n_parts, mixing, step)
+    for r in range(n_parts):
+        counts = {p: part.exchanges[r].count(p) for p in set(part.exchanges[r])}
+        assert counts == {p: 2 * n for p, n in EXCHANGES_PER_STEP.items()}, r
+    part.close()
+
+
+def test_one_ring_of_halo_is_not_enough(arrays):
+    """The comparison sees a halo that is too shallow."""
+    cfg = _config(False)
+    want = _single(arrays, cfg, 1)
+    part = partition.PartitionedDycore(arrays, cfg, 2, halo_rings=1)
+    part.step(1)
+    bad = _differing(part.get_state(), want[0])
+    assert bad.get("rho_u", 0) > 0 and bad.get("scalars", 0) > 0
+    part.close()
+
+
+def test_exchange_hook_failure_and_refusals(arrays):
+    """A hook that fails aborts the step with nothing published; a hooked
+    handle refuses graph capture and steps eagerly."""
+    lib = _lib.load()
+    cfg = _config(False)
+    drv = hexdyn.from_case(arrays_case(arrays), cfg)
+    before, _ = drv.get_state()
+    seen = []
+
+    def failing(user, point, nbufs, bufs, kinds):
+        seen.append(point)
+        return -1 if point == _lib.XCH_ACOUSTIC else 0
+
+    hook = _lib.EXCHANGE_HOOK(failing)
+    _lib.check(lib.hexdyn_set_exchange_hook(drv._handle, hook, None))
+    with pytest.raises(_lib.HexDynError, match="hook aborted step 1"):
+        drv.step_device(1)
+    assert seen == [_lib.XCH_STATE, _lib.XCH_DIAG, _lib.XCH_ACOUSTIC]
+    after, _ = drv.get_state()
+    for k in _lib.STATE_FIELDS:
+        assert differing_words(getattr(before, k), getattr(after, k)) == 0, k
+    assert lib.hexdyn_capture_graph(drv._handle, C.c_void_p(0)) == _lib.HEXDYN_E_STATE
+    # a hook that moves nothing leaves the step as it is (the callback object
+    # must outlive its registration)
+    noop = _lib.EXCHANGE_HOOK(lambda *a: 0)
+    _lib.check(lib.hexdyn_set_exchange_hook(drv._handle, noop, None))
+    drv.step_device(1)
+    _lib.check(lib.hexdyn_set_exchange_hook(drv._handle, _lib.EXCHANGE_HOOK(), None))
+    got, gside = drv.get_state()
+    want = _single(arrays, cfg, 1)[0]
+    assert _differing(({k: getattr(got, k) for k in _lib.STATE_FIELDS},
+                       {k: getattr(gside, k) for k in _lib.SIDECAR_FIELDS}), want) == {}
+    drv.capture_graph()   # no hook: the graph is allowed again
+    drv.close()

@@ -64,6 +64,8 @@ def parse() -> argparse.Namespace:
                     help="also time the uneven ensemble (24 x 10242-cell members at 1440 s + 16 x 40962-cell "
                          "members at 720 s) batched and looped")
     ap.add_argument("--batch-periods", type=int, default=4, help="timed 1440 s periods of the ensemble leg")
+    ap.add_argument("--partition-ranks", type=int, default=2,
+                    help="ranks of the partitioned-instance leg, emulated on one GPU (0 or 1: off)")
     ap.add_argument("--learned", default="on", choices=["on", "off"],
                     help="also train the learned corrector (shortened) and time the corrected path for half a day")
     return ap.parse_args()
@@ -450,6 +452,66 @@ def run_learned(args, plain_case) -> dict:
     }
 
 
+# ------------------------------------------------ partitioned single instance
+def run_partitioned(args, case, cfg) -> dict:
+    """One instance split over ``args.partition_ranks`` ranks emulated on this
+    GPU (``hexdyn.partition.PartitionedDycore``: a thread and a stream per
+    rank, halo exchanges as device copies at the step's exchange points).
+    The owned regions after one step are compared word for word with a
+    single instance's step from the same state, then steps are timed with
+    CUDA events on every rank's stream (max over ranks)."""
+    import numpy as np
+    import torch
+
+    import hexdyn
+    from hexdyn import _lib, partition
+    from hexdyn.case import case_arrays
+
+    arr = case_arrays(case)
+    ranks = args.partition_ranks
+    single = hexdyn.from_case(case, cfg)
+    single.step_device(1)
+    ref_state, ref_side = single.get_state()
+    single.close()
+    part = partition.PartitionedDycore(arr, cfg, ranks)
+    part.step(1)
+    got_state, got_side = part.get_state()
+    differing = 0
+    for name in _lib.STATE_FIELDS:
+        differing += int(np.count_nonzero(np.asarray(getattr(ref_state, name), np.float32).view(np.uint32)
+                                          != got_state[name].view(np.uint32)))
+    for name in _lib.SIDECAR_FIELDS:
+        differing += int(np.count_nonzero(np.asarray(getattr(ref_side, name), np.float32).view(np.uint32)
+                                          != got_side[name].view(np.uint32)))
+    n_before = len(part.exchanges[0])
+    part.step(1)   # warm-up
+    steps = 3
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ranks)]
+    for (e0, _), st in zip(ev, part.streams):
+        e0.record(st)
+    part.step(steps)
+    for (_, e1), st in zip(ev, part.streams):
+        e1.record(st)
+    torch.cuda.synchronize()
+    ms = max(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    exchanges = (len(part.exchanges[0]) - n_before) // (steps + 1)
+    lays = part.layouts
+    part.close()
+    dt = cfg.config_dt
+    return {
+        "metric": "simulated days/hour", "value": (dt / 86400.0) / (ms / 1000.0 / 3600.0), "ms_per_step": ms,
+        "steps": steps, "warmup": 1, "ranks": ranks, "emulated_on_one_gpu": True,
+        "halo_rings": partition.halo_rings_for(cfg), "exchanges_per_step": exchanges,
+        "owned_cells": [lay.n_owned["cell"] for lay in lays],
+        "halo_cells": [int(lay.l2g["cell"].size - lay.n_owned["cell"]) for lay in lays],
+        "halo_edges": [int(lay.l2g["edge"].size - lay.n_owned["edge"]) for lay in lays],
+        "owned_region_differing_words_vs_single_instance": differing,
+        "note": "ranks share one GPU here (eager steps, host hooks between launches): the number shows the path "
+                "running and its overhead, not multi-GPU scaling",
+    }
+
+
 # ------------------------------------------------------------------- arms
 def run_reference(args, rank: int) -> None:
     if rank != 0:
@@ -602,6 +664,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     batched = run_ensemble(args, stream, dist, world, rank, case) if args.batched == "on" else None
     learned = run_learned(args, case) if args.learned == "on" and args.level == 6 else None
+    partitioned = (run_partitioned(args, case, cfg)
+                   if args.partition_ranks > 1 and world == 1 and rank == 0 else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -635,6 +699,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "kernel_functions": merged,
             "batched": batched,
             "learned": learned,
+            "partitioned": partitioned,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

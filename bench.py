@@ -97,16 +97,19 @@ def kernel_bytes(name: str, C: int, E: int, V: int, L: int, T: int, maxE: int = 
         "k_euler_cell": el + 2 * ci + 5 * cl + conn_c,
         "k_hdiv": el + cl + conn_c,
         "k_edge_adv": 3 * el + cl + ci + adv,
-        "k_tend_u": 4 * el + ci + 3 * cl + conn_e + E * 24,
+        "k_tend_u": 6 * el + ci + 3 * cl + conn_e + E * 24,          # + the first substep's ru_p, ru_avg out
         "k_tend_cell": 5 * el + 5 * ci + 4 * cl + zb + conn_c,
         "k_vcoef": 9 * cl + 6 * cl + ci,
+        # the two launches below run only in builds without the acoustic fusions
         "k_ac_edge_first": 3 * el,                                 # tend_ru in; ru_p, ru_avg out
         "k_ac_edge": 7 * el + 6 * cl + conn_e,                     # damping of n-1 + update n
         "k_ac_edge_damp": 2 * el + 3 * cl + conn_e,                # damping only
         # (+ dss, rho_zz, w when the damping profile is not zero)
         "k_ac_cell_first": el + 10 * cl + 6 * ci + conn_c + (2 * cl + ci if damping else 0),  # old perts zero
         "k_ac_cell": el + 14 * cl + 8 * ci + conn_c + (2 * cl + ci if damping else 0),
-        "k_recover_edge": 7 * el + 3 * cl + conn_e,
+        # + the last substep's damping: ru_p out, rtpp_new and theta_m at both
+        # cells (rtpp_old only after a stage of several substeps: not counted)
+        "k_recover_edge": 8 * el + 5 * cl + conn_e,
         "k_recover_cell": el + 16 * cl + 7 * ci + zb + conn_c,       # + the next stage's hdiv
         "k_tr_edge": (tcl + tel) + el + adv,
         "k_tr_edge_mono": (tcl + tel) + el + adv,

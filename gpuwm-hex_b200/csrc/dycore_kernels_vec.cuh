@@ -513,7 +513,8 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
                           const float* __restrict__ rho, const float* __restrict__ pv_edge,
                           const float* __restrict__ ke, const float* __restrict__ hdiv,
                           const float* __restrict__ euler_ru, float* __restrict__ tend_ru,
-                          const float* __restrict__ phys_ru) {
+                          const float* __restrict__ phys_ru, float first_dts, float* __restrict__ ru_p0,
+                          float* __restrict__ ru_avg0) {
   HEX_VEC_PARALLEL(g.nE)
   const int e = ent, S = g.S;
   const int c0 = g.coe[2 * e], c1 = g.coe[2 * e + 1];
@@ -588,6 +589,15 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
     for (int j = 0; j < 4; ++j) out.a[j] = out.a[j] + pu.a[j];
   }
   st4m(tend_ru + e * S + k0, out, k0, 0, g.L);
+  if (ru_p0) {
+    // the stage's first acoustic substep starts from ru_p = ru_avg = dts x
+    // tend_ru (kv_ac_edge mode 0), formed here from the tendency in registers
+    V4 r;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) r.a[j] = first_dts * out.a[j];
+    st4m(ru_p0 + e * S + k0, r, k0, 0, g.L);
+    st4m(ru_avg0 + e * S + k0, r, k0, 0, g.L);
+  }
 }
 
 // theta vertical flux at interface j = k0 + d (hexcore/driver.py:1048-1076).
@@ -1024,18 +1034,38 @@ __global__ void HEX_VEC_BOUNDS kv_ac_edge(HexGeo g, int mode, int old_is_zero, f
 // hexcore/driver.py:3166-3292 stage recovery, edge part: ru = ru_s + ru_p,
 // u = 2 ru / (rho1 + rho2) (hexcore/driver.py:866), and the split mass-flux
 // average (hexcore/integration.py:27,58).
-__global__ void HEX_VEC_BOUNDS kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, const float* __restrict__ ru_p,
+// damp: the divergence damping of the stage's last acoustic substep
+// (kv_ac_edge mode 2: rtpp_new/rtpp_old its output/input, old_is_zero when
+// it was the first) is applied to ru_p here, stored, and recovered from.
+__global__ void HEX_VEC_BOUNDS kv_recover_edge(HexGeo g, const float* __restrict__ ru_s, float* ru_p,
                                 const float* __restrict__ ru_avg, const float* __restrict__ rp_s,
                                 const float* __restrict__ rho_pp, float* __restrict__ ru_out,
                                 float* __restrict__ u_out, float* __restrict__ flux_u, int flux_mode,
-                                float inv_steps, float inv_splits) {
+                                float inv_steps, float inv_splits, int damp, int old_is_zero, float inv_dts,
+                                const float* __restrict__ rtpp_new, const float* __restrict__ rtpp_old,
+                                const float* __restrict__ theta_s) {
   HEX_VEC_PARALLEL(g.nE)
   const int e = ent, S = g.S;
   const int jj = e * S + k0;
   const int i0 = g.coe[2 * e] * S + k0, i1 = g.coe[2 * e + 1] * S + k0;
+  V4 rp = ld4rw(ru_p + jj);
+  if (damp) {
+    const float damp_coef = g.smdiv_edge[e] * inv_dts;
+    const V4 n0 = ld4(rtpp_new + i0), n1 = ld4(rtpp_new + i1);
+    const V4 o0 = old_is_zero ? v4zero() : ld4(rtpp_old + i0);
+    const V4 o1 = old_is_zero ? v4zero() : ld4(rtpp_old + i1);
+    const V4 t0 = ld4(theta_s + i0), t1 = ld4(theta_s + i1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float d0 = n0.a[j] - o0.a[j];
+      const float d1 = n1.a[j] - o1.a[j];
+      rp.a[j] = rp.a[j] + damp_coef * (d0 - d1) * (1.0f - 0.0f) / (t0.a[j] + t1.a[j]);
+    }
+    st4m(ru_p + jj, rp, k0, 0, g.L);
+  }
   const V4 a0 = ld4(rp_s + i0), a1 = ld4(rp_s + i1), b0 = ld4(rho_pp + i0), b1 = ld4(rho_pp + i1);
   const V4 c0 = ld4(g.rho_base + i0), c1 = ld4(g.rho_base + i1);
-  const V4 rs = ld4(ru_s + jj), rp = ld4(ru_p + jj);
+  const V4 rs = ld4(ru_s + jj);
   V4 ru, uo;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {

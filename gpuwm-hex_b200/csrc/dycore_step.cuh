@@ -1,5 +1,15 @@
 #include <initializer_list>
 #include <utility>
+// The first acoustic substep's start values (ru_p = ru_avg = dts tend_ru)
+// formed by the momentum tendency, and the last substep's divergence
+// damping applied by the edge recovery, instead of two kv_ac_edge launches
+// per RK stage (the same operations on the same words).
+#ifndef HEX_FUSE_AC_FIRST
+#define HEX_FUSE_AC_FIRST 1
+#endif
+#ifndef HEX_FUSE_AC_DAMP
+#define HEX_FUSE_AC_DAMP 1
+#endif
 // Step orchestration: hexcore/driver.py:3314 DryDycoreDriver.step with the
 // v8.4.1 subcycle of hexcore/driver.py:2710, as a fixed sequence of kernel
 // launches on one stream (capturable into one CUDA graph).
@@ -278,7 +288,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
       L.lpv("k_tend_u", g.nE, 1, g.rayleigh_levels ? kv_tend_u<true> : kv_tend_u<false>, g, (const float*)cs->u,
             (const float*)cur->rho_w, (const float*)cur->rho, (const float*)w.pv_edge, (const float*)w.ke,
             (const float*)w.hdiv, saved_ru, w.tend_ru,
-            (const float*)((phys & HEXDYN_PHYS_RHO_U) ? ctx.phys_ru : nullptr));
+            (const float*)((phys & HEXDYN_PHYS_RHO_U) ? ctx.phys_ru : nullptr), dts,
+            HEX_FUSE_AC_FIRST ? w.ru_p : nullptr, HEX_FUSE_AC_FIRST ? w.ru_avg : nullptr);
       if (stg.stage == 2 && ctx.order == 3) {  // hexcore/driver.py:2894
         LPG(L, "k_vcoef", g.nC, sm_vcoef, sm_vcoef_v, vcoef, g, stg.dts2, (const float*)s_in->exner, (const float*)cs->theta_m,
              (const float*)cs->rtheta_p, (const float*)w.cqw, (const float*)w.qtot, w.cofwr, w.cofwz, w.coftz,
@@ -299,6 +310,8 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         const float* old_rt = w.rtpp[(n - 1) & 1];
         float* new_rt = w.rtpp[n & 1];
         if (n == 1) {
+          // (with HEX_FUSE_AC_FIRST the momentum tendency already formed them)
+          if (!HEX_FUSE_AC_FIRST)
           LPSN(L, "k_ac_edge_first", g.nE, 1, ac_edge, g, 0, 1, dts, inv_dts, (const float*)w.tend_ru, (const float*)new_rt,
                old_rt, (const float*)w.rho_pp, (const float*)s_in->theta_m, (const float*)s_in->exner,
                (const float*)w.cqu, w.ru_p, w.ru_avg);
@@ -319,19 +332,22 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
         exchange(HEXDYN_XCH_ACOUSTIC, {{w.rho_pp, KC}, {new_rt, KC}, {w.rw_p, KC}, {w.ww_avg, KC}, {w.ru_p, KE},
                                        {w.ru_avg, KE}});
       }
-      {
-        const int n = stg.acoustic_steps;
-        LPSN(L, "k_ac_edge_damp", g.nE, 1, ac_edge, g, 2, n == 1 ? 1 : 0, dts, inv_dts, (const float*)w.tend_ru,
-             (const float*)w.rtpp[n & 1], (const float*)w.rtpp[(n - 1) & 1], (const float*)w.rho_pp,
+      const int n_last = stg.acoustic_steps;
+      if (!HEX_FUSE_AC_DAMP) {
+        LPSN(L, "k_ac_edge_damp", g.nE, 1, ac_edge, g, 2, n_last == 1 ? 1 : 0, dts, inv_dts, (const float*)w.tend_ru,
+             (const float*)w.rtpp[n_last & 1], (const float*)w.rtpp[(n_last - 1) & 1], (const float*)w.rho_pp,
              (const float*)s_in->theta_m, (const float*)s_in->exner, (const float*)w.cqu, w.ru_p, w.ru_avg);
       }
       const float* rtpp_final = w.rtpp[stg.acoustic_steps & 1];
       const float inv_steps = 1.0f / (float)stg.acoustic_steps;
       const float inv_splits = 1.0f / (float)ctx.split_steps;
       const int fm = stg.stage == 3 ? flux_mode : 0;
-      LPS(L, g.nE, 1, recover_edge, g, (const float*)saved->rho_u, (const float*)w.ru_p,
+      // (with HEX_FUSE_AC_DAMP the last substep's divergence damping of
+      // ru_p runs inside the edge recovery)
+      LPS(L, g.nE, 1, recover_edge, g, (const float*)saved->rho_u, w.ru_p,
            (const float*)w.ru_avg, (const float*)s_in->rho_p, (const float*)w.rho_pp, o.rho_u, so.u, w.flux_u,
-           fm, inv_steps, inv_splits);
+           fm, inv_steps, inv_splits, HEX_FUSE_AC_DAMP, n_last == 1 ? 1 : 0, inv_dts,
+           (const float*)w.rtpp[n_last & 1], (const float*)w.rtpp[(n_last - 1) & 1], (const float*)s_in->theta_m);
       // the cell recovery and the diagnostics of the new u share no array
       L.region = 4;
       L.fork();

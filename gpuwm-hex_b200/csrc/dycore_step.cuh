@@ -10,6 +10,9 @@
 #ifndef HEX_FUSE_AC_DAMP
 #define HEX_FUSE_AC_DAMP 1
 #endif
+#ifndef HEX_SKIP_FINAL_DIAG
+#define HEX_SKIP_FINAL_DIAG 1
+#endif
 // Step orchestration: hexcore/driver.py:3314 DryDycoreDriver.step with the
 // v8.4.1 subcycle of hexcore/driver.py:2710, as a fixed sequence of kernel
 // launches on one stream (capturable into one CUDA graph).
@@ -356,7 +359,9 @@ cudaError_t run_step(HexCtx& ctx, const HexState& in, const HexSide& side_in, co
            (const float*)w.rw_p, (const float*)w.ww_avg, (const float*)o.rho_u, o, so, w.flux_w, fm, inv_steps,
            inv_splits, w.flag, w.hdiv);
       L.side();
-      diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
+      // the step's last stage needs none: nothing after it reads them, and
+      // the next step forms them from the same u at its start
+      if (!(last && si == 2) || !HEX_SKIP_FINAL_DIAG) diagnostics(L, so.u, stg.stage == 3 ? 1 : 0);
       L.join();
       exchange(HEXDYN_XCH_STATE, {{o.rho, KC}, {o.rho_theta, KC}, {o.rho_u, KE}, {o.rho_w, KC}, {so.theta_m, KC},
                                   {so.exner, KC}, {so.rho_p, KC}, {so.rtheta_p, KC}, {so.pressure_p, KC},

@@ -34,6 +34,9 @@
 #ifndef HEX_TEND_U_MIN_BLOCKS
 #define HEX_TEND_U_MIN_BLOCKS 6
 #endif
+#ifndef HEX_EDGE_ADV_MIN_BLOCKS
+#define HEX_EDGE_ADV_MIN_BLOCKS HEX_VEC_MIN_BLOCKS
+#endif
 #ifndef HEX_TR_EDGE_MIN_BLOCKS
 #define HEX_TR_EDGE_MIN_BLOCKS 2
 #endif
@@ -63,6 +66,20 @@
 // together.  HEX_GATHER_UNROLL sets the unroll factor (0: the compiler's choice).
 #ifndef HEX_GATHER_UNROLL
 #define HEX_GATHER_UNROLL 2
+#endif
+// Per-kernel unroll of the neighbour loop (default HEX_GATHER_UNROLL).
+// Swept on the x1.40962 workload: the theta/w edge values run fastest
+// unrolled by five (55.5 vs 58.3 us per launch; three 57.7); the momentum
+// tendency by four or five (with 64 registers) and the tracer edge values by
+// three or five were slower than two.
+#ifndef HEX_TEND_U_UNROLL
+#define HEX_TEND_U_UNROLL HEX_GATHER_UNROLL
+#endif
+#ifndef HEX_TR_EDGE_UNROLL
+#define HEX_TR_EDGE_UNROLL HEX_GATHER_UNROLL
+#endif
+#ifndef HEX_EDGE_ADV_UNROLL
+#define HEX_EDGE_ADV_UNROLL 5
 #endif
 #define HEX_PRAGMA(x) _Pragma(#x)
 #define HEX_UNROLL_N(n) HEX_PRAGMA(unroll n)
@@ -430,7 +447,7 @@ __global__ void HEX_VEC_BOUNDS kv_hdiv(HexGeo g, const float* __restrict__ ru, f
 
 // Third-order edge values of theta_m (levels) and w (interfaces):
 // hexcore/driver.py:1023-1034 and :1159-1172.
-__global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ ru, const float* __restrict__ theta,
+__global__ void __launch_bounds__(256, HEX_EDGE_ADV_MIN_BLOCKS) kv_edge_adv(HexGeo g, const float* __restrict__ ru, const float* __restrict__ theta,
                             const float* __restrict__ w, float* __restrict__ edge_theta,
                             float* __restrict__ edge_w) {
   HEX_VEC_PARALLEL(g.nE)
@@ -455,7 +472,7 @@ __global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ r
     nw[j] = signbit(g.fzm[k] * r.a[j] + g.fzp[k] * rprev);
   }
   V4 at = v4zero(), aw = v4zero();
-  HEX_GATHER
+  HEX_UNROLL_N(HEX_EDGE_ADV_UNROLL)
   for (int s = 0; s < n; ++s) {
     const int cs = cells[s] * S + k0;
     const float A = a1[s], X = g.coef3 * a3[s];
@@ -478,7 +495,7 @@ __global__ void HEX_VEC_BOUNDS kv_edge_adv(HexGeo g, const float* __restrict__ r
     cw[j] = g.coef3 * copysignf(1.0f, rui);
   }
   V4 at = v4zero(), aw = v4zero();
-  HEX_GATHER
+  HEX_UNROLL_N(HEX_EDGE_ADV_UNROLL)
   for (int s = 0; s < n; ++s) {
     const int cs = cells[s] * S + k0;
     const float A = a1[s], B = a3[s];
@@ -526,7 +543,7 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
   const int n = g.neoe[e];
   const V4 pve = ld4(pv_edge + e * S + k0);
   V4 q = v4zero();
-  HEX_GATHER
+  HEX_UNROLL_N(HEX_TEND_U_UNROLL)
   for (int s = 0; s < n; ++s) {
     const int nb = g.eoe[e * g.maxE2 + s];
     const float w = g.weights[e * g.maxE2 + s];
@@ -547,7 +564,7 @@ __global__ void __launch_bounds__(256, HEX_TEND_U_MIN_BLOCKS) kv_tend_u(HexGeo g
   for (int j = 0; j < 4; ++j) need = need || (k0 + j < g.L && !(fabsf(q.a[j]) > 0.0f));
   if (need) {
     const float fe = g.f_edge[e];
-    HEX_GATHER
+    HEX_UNROLL_N(HEX_TEND_U_UNROLL)
     for (int s = 0; s < n; ++s) {
       const int nb = g.eoe[e * g.maxE2 + s];
       const float w = g.weights[e * g.maxE2 + s];
@@ -1288,7 +1305,7 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
           for (int j = 0; j < 4; ++j) res[t].a[j] = w[j] * qv.a[j];
         }
     }
-    HEX_GATHER
+    HEX_UNROLL_N(HEX_TR_EDGE_UNROLL)
     for (int s = 1; s < 10; ++s) {
       const float* qc = qg + cells[s] * S;
       HEX_TR_WEIGHTS(s)
@@ -1307,7 +1324,7 @@ __global__ void __launch_bounds__(256, HEX_TR_EDGE_MIN_BLOCKS) kv_tr_edge(HexGeo
   } else {
 #pragma unroll
     for (int t = 0; t < TG; ++t) res[t] = v4zero();
-    HEX_GATHER
+    HEX_UNROLL_N(HEX_TR_EDGE_UNROLL)
     for (int s = 0; s < n; ++s) {
       const float* qc = qg + cells[s] * S;
       HEX_TR_WEIGHTS(s)

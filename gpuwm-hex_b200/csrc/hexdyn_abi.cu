@@ -1301,6 +1301,108 @@ int hexdyn_set_exchange_hook(HexDynHandle* h, HexDynExchangeHook hook, void* use
   return HEXDYN_OK;
 }
 
+// Halo rows of a partitioned instance: one launch moves the chosen rows of
+// every buffer of an exchange point into one packed array or back.  Packed
+// layout: buffer by buffer, block by block (tracer blocks), row by row, the
+// S words of each row.
+#define HEX_HALO_MAX 24
+struct HexHaloBufs {
+  float* p[HEX_HALO_MAX];
+  const int* idx[HEX_HALO_MAX];
+  int rows[HEX_HALO_MAX];    // rows of one block of the buffer (cells or edges)
+  int nrows[HEX_HALO_MAX];   // rows moved
+  long long off[HEX_HALO_MAX + 1];  // start of each buffer in the packed array (16-byte units)
+  int n;
+};
+
+__global__ void k_halo_rows(HexHaloBufs hb, int S4, float4* packed, int unpack) {
+  const long long total = hb.off[hb.n];
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int b = 0;
+    while (t >= hb.off[b + 1]) ++b;
+    const long long u = t - hb.off[b];
+    const int l = (int)(u % S4);
+    const long long r = u / S4;
+    const int i = (int)(r % hb.nrows[b]);
+    const long long blk = r / hb.nrows[b];
+    const int row = hb.idx[b][i];
+    if (row < 0 || row >= hb.rows[b]) continue;  // the host checked the lists; never touch memory outside
+    float4* cell = reinterpret_cast<float4*>(hb.p[b]) + (blk * hb.rows[b] + row) * S4 + l;
+    if (unpack)
+      *cell = packed[t];
+    else
+      packed[t] = *cell;
+  }
+}
+
+static int halo_setup(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                      int n_cell_rows, const int* edge_rows, int n_edge_rows, HexHaloBufs& hb) {
+  if (!h || (nbuf > 0 && (!bufs || !kinds))) return fail(HEXDYN_E_ARG, "NULL argument");
+  if (nbuf < 0 || nbuf > HEX_HALO_MAX) return fail(HEXDYN_E_ARG, "nbuf %d outside [0, %d]", nbuf, HEX_HALO_MAX);
+  if (n_cell_rows < 0 || n_edge_rows < 0) return fail(HEXDYN_E_ARG, "negative row count");
+  if ((n_cell_rows > 0 && !cell_rows) || (n_edge_rows > 0 && !edge_rows)) return fail(HEXDYN_E_ARG, "NULL row list");
+  const HexCtx& c = h->ctx;
+  hb = HexHaloBufs{};
+  hb.n = nbuf;
+  for (int b = 0; b < nbuf; ++b) {
+    const int k = kinds[b];
+    if (k != HEXDYN_KIND_CELL && k != HEXDYN_KIND_EDGE && k != HEXDYN_KIND_TRACER)
+      return fail(HEXDYN_E_ARG, "buffer %d: unknown kind %d", b, k);
+    if (!bufs[b] || (reinterpret_cast<uintptr_t>(bufs[b]) & 15))
+      return fail(HEXDYN_E_ARG, "buffer %d: NULL or not 16-byte aligned", b);
+    const bool edge = k == HEXDYN_KIND_EDGE;
+    const int blocks = k == HEXDYN_KIND_TRACER ? std::max(1, c.n_scalars) : 1;
+    hb.p[b] = bufs[b];
+    hb.idx[b] = edge ? edge_rows : cell_rows;
+    hb.rows[b] = edge ? c.geo.nE : c.geo.nC;
+    hb.nrows[b] = edge ? n_edge_rows : n_cell_rows;
+    hb.off[b + 1] = hb.off[b] + (long long)blocks * hb.nrows[b] * (c.geo.S / 4);
+  }
+  return HEXDYN_OK;
+}
+
+size_t hexdyn_halo_words(HexDynHandle* h, int nbuf, const int* kinds, int n_cell_rows, int n_edge_rows) {
+  if (!h || nbuf < 0 || nbuf > HEX_HALO_MAX || (nbuf > 0 && !kinds)) return 0;
+  size_t words = 0;
+  for (int b = 0; b < nbuf; ++b) {
+    const int blocks = kinds[b] == HEXDYN_KIND_TRACER ? std::max(1, h->ctx.n_scalars) : 1;
+    words += (size_t)blocks * (kinds[b] == HEXDYN_KIND_EDGE ? n_edge_rows : n_cell_rows) * h->ctx.geo.S;
+  }
+  return words;
+}
+
+static int halo_move(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                     int n_cell_rows, const int* edge_rows, int n_edge_rows, float* packed, void* stream,
+                     int unpack) {
+  HexHaloBufs hb;
+  const int rc = halo_setup(h, nbuf, bufs, kinds, cell_rows, n_cell_rows, edge_rows, n_edge_rows, hb);
+  if (rc != HEXDYN_OK) return rc;
+  const long long total = hb.off[nbuf];
+  if (total == 0) return HEXDYN_OK;
+  if (!packed || (reinterpret_cast<uintptr_t>(packed) & 15))
+    return fail(HEXDYN_E_ARG, "packed array NULL or not 16-byte aligned");
+  const int threads = 256;
+  const long long want = (total + threads - 1) / threads;
+  const int grid = (int)std::min<long long>(want, 148LL * 8);
+  k_halo_rows<<<grid, threads, 0, (cudaStream_t)stream>>>(hb, h->ctx.geo.S / 4, reinterpret_cast<float4*>(packed),
+                                                            unpack);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "halo rows");
+  return HEXDYN_OK;
+}
+
+int hexdyn_halo_pack(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                     int n_cell_rows, const int* edge_rows, int n_edge_rows, float* packed, void* stream) {
+  return halo_move(h, nbuf, bufs, kinds, cell_rows, n_cell_rows, edge_rows, n_edge_rows, packed, stream, 0);
+}
+
+int hexdyn_halo_unpack(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                       int n_cell_rows, const int* edge_rows, int n_edge_rows, const float* packed, void* stream) {
+  return halo_move(h, nbuf, bufs, kinds, cell_rows, n_cell_rows, edge_rows, n_edge_rows,
+                   const_cast<float*>(packed), stream, 1);
+}
+
 int hexdyn_physics_buffer(HexDynHandle* h, int which, void** device_ptr) {
   if (!h || !device_ptr) return fail(HEXDYN_E_ARG, "NULL argument");
   HexCtx& c = h->ctx;

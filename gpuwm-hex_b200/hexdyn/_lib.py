@@ -118,6 +118,11 @@ EXPORTS = {
     "hexdyn_set_stage_hook": (C.c_int, [C.c_void_p, STAGE_HOOK, C.c_void_p]),
     "hexdyn_physics_buffer": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "hexdyn_set_exchange_hook": (C.c_int, [C.c_void_p, EXCHANGE_HOOK, C.c_void_p]),
+    "hexdyn_halo_words": (C.c_size_t, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int]),
+    "hexdyn_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
+                                   C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "hexdyn_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
+                                     C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "hexdyn_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "hexdyn_destroy": (C.c_int, [C.c_void_p]),
 }

@@ -32,13 +32,18 @@ Two runners share the layouts and plans:
   buffers, ordered by CUDA events and a host barrier (no kernel waits on
   another kernel);
 * ``RankDycore`` -- one rank per process and GPU over ``torch.distributed``
-  (NCCL): exchanges are ``batch_isend_irecv`` of the packed owned rows into
-  the receiver's halo rows (``exchange_rows``), posted in the same order on
-  every rank.
+  (NCCL): at each point one packed array of owned rows per peer is sent
+  and one received (``exchange_packed``), posted in the same order on every
+  rank.
+
+Rows move with the library's one-launch kernels (``hexdyn_halo_pack`` /
+``hexdyn_halo_unpack``): every buffer of an exchange point in one launch per
+peer and direction.
 """
 
 from __future__ import annotations
 
+import ctypes as C
 import threading
 from dataclasses import dataclass, field
 from typing import Any
@@ -49,7 +54,6 @@ from . import _lib
 from .reorder import _CASE, _MESH_ROWS, _PASS, _sizes
 
 ENTITIES = ("cell", "edge", "vertex")
-KIND_ENTITY = {_lib.KIND_CELL: "cell", _lib.KIND_EDGE: "edge", _lib.KIND_TRACER: "cell"}
 
 
 def cell_owners(n_cells: int, n_parts: int) -> np.ndarray:
@@ -208,53 +212,135 @@ def plans(lays: list[Layout]) -> list[ExchangePlan]:
     return [ExchangePlan.build(lays, r) for r in range(len(lays))]
 
 
-def exchange_rows(plan: ExchangePlan, buffers: list, group=None, index_cache: dict | None = None) -> None:
-    """One exchange point over ``torch.distributed``: every buffer is a
-    ``(blocks, rows, S)`` tensor with its kind (``cell`` / ``edge``); the owned
-    rows each peer needs are packed and sent, the received rows written into
-    this rank's halo.  All sends and receives of the point are posted
-    together (``batch_isend_irecv``) in one order shared by every rank:
-    buffers in the order given, peers ascending."""
+KINDS = ("cell", "edge")
+
+
+class TorchRows:
+    """The buffers of one exchange point as ``(blocks, rows, S)`` tensors of
+    any device, packed and unpacked with torch indexing: buffer by buffer,
+    the rows of its kind (cell rows for cell and tracer buffers) in list
+    order.  The device runners move the same rows with the library's
+    one-launch kernels (``DeviceRows``)."""
+
+    def __init__(self, buffers: list):
+        self.buffers = buffers   # [(tensor, kind)]
+
+    def words(self, rows: dict) -> int:
+        return sum(int(b.shape[0]) * len(rows[k]) * int(b.shape[2]) for b, k in self.buffers if k in rows)
+
+    def pack(self, key, rows: dict, out) -> None:
+        import torch
+
+        parts = [b[:, torch.as_tensor(rows[k], dtype=torch.long, device=b.device)].reshape(-1)
+                 for b, k in self.buffers if k in rows]
+        if parts:
+            out.copy_(torch.cat(parts))
+
+    def unpack(self, key, rows: dict, packed) -> None:
+        import torch
+
+        off = 0
+        for b, k in self.buffers:
+            if k not in rows:
+                continue
+            n = int(b.shape[0]) * len(rows[k]) * int(b.shape[2])
+            idx = torch.as_tensor(rows[k], dtype=torch.long, device=b.device)
+            b[:, idx] = packed[off:off + n].view(int(b.shape[0]), len(rows[k]), int(b.shape[2]))
+            off += n
+
+
+class DeviceRows:
+    """The buffers of one exchange point as the library hands them to the
+    hook (device pointers and kinds), moved by ``hexdyn_halo_pack`` /
+    ``hexdyn_halo_unpack``: one launch per peer and direction."""
+
+    def __init__(self, driver, nbuf: int, bufs, kinds, stream, index_cache: dict):
+        self.lib = _lib.load()
+        self.handle = driver._handle
+        self.nbuf = nbuf
+        self.ptrs = (C.c_void_p * max(1, nbuf))(*[bufs[i] for i in range(nbuf)])
+        self.kinds = (C.c_int * max(1, nbuf))(*[kinds[i] for i in range(nbuf)])
+        self.stream = stream
+        self.cache = index_cache
+
+    def _rows(self, key, kind, rows):
+        import torch
+
+        if kind not in rows:
+            return None, 0
+        t = self.cache.get((key, kind))
+        if t is None:
+            t = self.cache[(key, kind)] = torch.as_tensor(np.asarray(rows[kind], dtype=np.int32), device="cuda")
+        return C.c_void_p(t.data_ptr()), int(t.numel())
+
+    def words(self, rows: dict) -> int:
+        n = {k: len(rows[k]) if k in rows else 0 for k in KINDS}
+        return int(self.lib.hexdyn_halo_words(self.handle, self.nbuf, self.kinds, n["cell"], n["edge"]))
+
+    def _move(self, fn, key, rows, packed) -> None:
+        (cp, cn), (ep, en) = self._rows(key, "cell", rows), self._rows(key, "edge", rows)
+        stream = C.c_void_p(int(getattr(self.stream, "cuda_stream", self.stream)))
+        _lib.check(fn(self.handle, self.nbuf, self.ptrs, self.kinds, cp, cn, ep, en, C.c_void_p(packed.data_ptr()),
+                      stream))
+
+    def pack(self, key, rows: dict, out) -> None:
+        self._move(self.lib.hexdyn_halo_pack, key, rows, out)
+
+    def unpack(self, key, rows: dict, packed) -> None:
+        self._move(self.lib.hexdyn_halo_unpack, key, rows, packed)
+
+
+def exchange_packed(plan: ExchangePlan, packer, group=None, alloc=None) -> None:
+    """One exchange point over ``torch.distributed``: for every peer (in
+    ascending order, the same on every rank) the owned rows it needs, of
+    every buffer of the point, are packed into one array and sent; the rows
+    received from it are unpacked into this rank's halo.  All sends and
+    receives of the point are posted together (``batch_isend_irecv``).
+    ``packer``: ``TorchRows`` or ``DeviceRows``; ``alloc(key, words)``
+    returns a float32 buffer of at least ``words`` (default: a new tensor on
+    the packer's device)."""
     import torch
     import torch.distributed as dist
 
-    cache = {} if index_cache is None else index_cache
+    def new(key, n):
+        dev = packer.buffers[0][0].device if isinstance(packer, TorchRows) else "cuda"
+        return torch.empty(n, dtype=torch.float32, device=dev)
 
-    def idx(key, rows, device):
-        t = cache.get((key, str(device)))
-        if t is None:
-            t = cache[(key, str(device))] = torch.as_tensor(rows, dtype=torch.long, device=device)
-        return t
-
-    ops, unpack = [], []
-    for buf, kind in buffers:
-        for q in plan.peers():
-            rows = plan.send.get((q, kind))
-            if rows is not None:
-                packed = buf.index_select(1, idx(("send", q, kind), rows, buf.device)).contiguous()
-                ops.append(dist.P2POp(dist.isend, packed, q, group=group))
-            pair = plan.recv.get((q, kind))
-            if pair is not None:
-                tmp = torch.empty((buf.shape[0], pair[0].size, buf.shape[2]), dtype=buf.dtype, device=buf.device)
-                ops.append(dist.P2POp(dist.irecv, tmp, q, group=group))
-                unpack.append((buf, idx(("recv", q, kind), pair[0], buf.device), tmp))
+    alloc = alloc or new
+    ops, pending = [], []
+    for q in plan.peers():
+        send = {k: plan.send[(q, k)] for k in KINDS if (q, k) in plan.send}
+        if send:
+            n = packer.words(send)
+            buf = alloc(("send", q), n)[:n]
+            packer.pack(("send", q), send, buf)
+            ops.append(dist.P2POp(dist.isend, buf, q, group=group))
+        recv = {k: plan.recv[(q, k)][0] for k in KINDS if (q, k) in plan.recv}
+        if recv:
+            n = packer.words(recv)
+            buf = alloc(("recv", q), n)[:n]
+            ops.append(dist.P2POp(dist.irecv, buf, q, group=group))
+            pending.append((q, recv, buf))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
-    for buf, rows, tmp in unpack:
-        buf.index_copy_(1, rows, tmp)
+    for q, recv, buf in pending:
+        packer.unpack(("recv", q), recv, buf)
 
 
-def _view(ptr: int, kind: int, drv) -> Any:
-    """A library buffer of ``kind`` as a ``(blocks, rows, S)`` CUDA tensor."""
-    import torch
+class _Buffers:
+    """Growing float32 device buffers by key (packed halo rows)."""
 
-    from .driver import _CudaArray
+    def __init__(self):
+        self.bufs: dict = {}
 
-    s = drv.sizes
-    rows = s["n_edges"] if kind == _lib.KIND_EDGE else s["n_cells"]
-    blocks = s["n_scalars"] if kind == _lib.KIND_TRACER else 1
-    return torch.as_tensor(_CudaArray(ptr, (blocks, rows, drv.level_stride), drv), device="cuda")
+    def __call__(self, key, words: int):
+        import torch
+
+        b = self.bufs.get(key)
+        if b is None or b.numel() < words:
+            b = self.bufs[key] = torch.empty(max(1, words), dtype=torch.float32, device="cuda")
+        return b
 
 
 def gather_owned(lays: list[Layout], parts: list[tuple[Any, Any]]) -> tuple[dict, dict]:
@@ -308,47 +394,44 @@ class PartitionedDycore:
         self.device = torch.cuda.current_device()
         self.timeout = barrier_timeout
         self._barrier = threading.Barrier(n_parts)
-        self._bufs: list[list] = [[] for _ in range(n_parts)]
+        self._points: list = [None] * n_parts
         self._ready = [torch.cuda.Event() for _ in range(n_parts)]
         self._copied = [torch.cuda.Event() for _ in range(n_parts)]
         self._index: dict = {}
+        self._packed = _Buffers()
         self._errors: list[BaseException] = []
         self.exchanges: list[list[int]] = [[] for _ in range(n_parts)]
         self._hooks = [_lib.EXCHANGE_HOOK(self._hook_for(r)) for r in range(n_parts)]
-        for r in range(n_parts):   # the device index tensors, made once
-            for (q, kind), (mine, theirs) in self.plans[r].recv.items():
-                self._rows(("recv", r, q, kind), mine)
-                self._rows(("own", r, q, kind), theirs)
-
-    def _rows(self, key, rows):
-        import torch
-
-        t = self._index.get(key)
-        if t is None:
-            t = self._index[key] = torch.as_tensor(rows, dtype=torch.long, device="cuda")
-        return t
+        # rows rank r receives from q: its halo rows and q's owned rows
+        self._recv = [{q: ({k: self.plans[r].recv[(q, k)][0] for k in KINDS if (q, k) in self.plans[r].recv},
+                           {k: self.plans[r].recv[(q, k)][1] for k in KINDS if (q, k) in self.plans[r].recv})
+                       for q in range(n_parts)} for r in range(n_parts)]
 
     def _hook_for(self, r: int):
         import torch
 
         def hook(user, point, nbufs, bufs, kinds):
             try:
-                drv, st = self.drivers[r], self.streams[r]
-                self._bufs[r] = [(_view(bufs[i], kinds[i], drv), KIND_ENTITY[kinds[i]]) for i in range(nbufs)]
+                st = self.streams[r]
+                self._points[r] = DeviceRows(self.drivers[r], nbufs, bufs, kinds, st, self._index)
                 self._ready[r].record(st)
                 self._barrier.wait(self.timeout)
                 for q in range(self.n_parts):
                     if q != r:
                         st.wait_event(self._ready[q])
-                with torch.cuda.stream(st):
-                    for i, (dst, kind) in enumerate(self._bufs[r]):
-                        for q in range(self.n_parts):
-                            pair = self.plans[r].recv.get((q, kind))
-                            if pair is None:
-                                continue
-                            src = self._bufs[q][i][0]
-                            dst.index_copy_(1, self._index[("recv", r, q, kind)],
-                                            src.index_select(1, self._index[("own", r, q, kind)]))
+                mine = self._points[r]
+                for q in range(self.n_parts):
+                    halo, owned = self._recv[r][q]
+                    if not halo:
+                        continue
+                    # q's owned rows packed with q's handle, unpacked into r's
+                    # halo with r's, both on r's stream
+                    theirs = self._points[q]
+                    src = DeviceRows(self.drivers[q], theirs.nbuf, theirs.ptrs, theirs.kinds, st, self._index)
+                    n = mine.words(halo)
+                    packed = self._packed((r, q), n)
+                    src.pack(("own", r, q), owned, packed)
+                    mine.unpack(("halo", r, q), halo, packed)
                 self._copied[r].record(st)
                 self._barrier.wait(self.timeout)
                 for q in range(self.n_parts):
@@ -423,6 +506,7 @@ class RankDycore:
         self.stream = torch.cuda.Stream()
         self.driver = _driver(local_arrays(arr, self.layout), config, stream=self.stream)
         self._index: dict = {}
+        self._packed = _Buffers()
         self._error: BaseException | None = None
         self._hook = _lib.EXCHANGE_HOOK(self._exchange)
 
@@ -430,9 +514,9 @@ class RankDycore:
         import torch
 
         try:
-            buffers = [(_view(bufs[i], kinds[i], self.driver), KIND_ENTITY[kinds[i]]) for i in range(nbufs)]
             with torch.cuda.stream(self.stream):
-                exchange_rows(self.plan, buffers, self.group, self._index)
+                exchange_packed(self.plan, DeviceRows(self.driver, nbufs, bufs, kinds, self.stream, self._index),
+                                self.group, self._packed)
             return 0
         except BaseException as exc:  # noqa: BLE001 - re-raised by step()
             self._error = exc

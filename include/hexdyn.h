@@ -305,6 +305,24 @@ int hexdyn_physics_buffer(HexDynHandle* h, int which, void** device_ptr);
 typedef int (*HexDynExchangeHook)(void* user, int point, int nbufs, float* const* bufs, const int* kinds);
 int hexdyn_set_exchange_hook(HexDynHandle* h, HexDynExchangeHook hook, void* user);
 
+/* Halo rows of an exchange point in one launch (no counterpart in the
+ * reference, whose executor packs each field with a NumPy/CuPy fancy index,
+ * hexcore/partition_executor_v841.py): hexdyn_halo_pack copies the rows
+ * `cell_rows` (cell and tracer buffers) and `edge_rows` (edge buffers) --
+ * device int32 lists of local row indices -- of the `nbuf` (<= 24) buffers of
+ * a hook call, padded layout and shapes of handle `h`, into `packed`;
+ * hexdyn_halo_unpack writes them back from `packed`.  Packed layout: buffer
+ * by buffer, tracer block by block, row by row, S words per row;
+ * hexdyn_halo_words gives its size in floats.  `packed` and every buffer
+ * 16-byte aligned; row indices outside the buffer are skipped.  A rank packs
+ * the owned rows its peer needs (with its own handle), the peer unpacks them
+ * into its halo rows (with its handle), in the same buffer order. */
+size_t hexdyn_halo_words(HexDynHandle* h, int nbuf, const int* kinds, int n_cell_rows, int n_edge_rows);
+int hexdyn_halo_pack(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                     int n_cell_rows, const int* edge_rows, int n_edge_rows, float* packed, void* stream);
+int hexdyn_halo_unpack(HexDynHandle* h, int nbuf, float* const* bufs, const int* kinds, const int* cell_rows,
+                       int n_cell_rows, const int* edge_rows, int n_edge_rows, const float* packed, void* stream);
+
 /* Bind caller-owned device buffers (padded layout, 16-byte aligned, every
  * field; replaces the reference's DeviceAtmosphere handed to the driver,
  * hexcore/cuda_driver.py:5419) as the current state

@@ -9,7 +9,8 @@ send/receive pairs (``hexcore/partition_nccl_transport_v841.py``):
   is owned by exactly one other rank, which sends it;
 * the local case arrays are a valid case (connectivity in range, slots kept
   in order) and, at one rank, the global case itself;
-* over ``torch.distributed`` (gloo, two and three ranks) one exchange fills
+* over ``torch.distributed`` (gloo, two and three ranks) one exchange
+  (``exchange_packed``: one packed array per peer and direction) fills
   every halo row of cell, edge and tracer buffers with its owner's value and
   leaves every owned row alone.
 
@@ -128,9 +129,9 @@ def _exchange_worker(rank, world, port, result_dir):
             start[:, lay.n_owned[kind]:] = -7.0   # halo rows not yet received
             bufs.append((torch.from_numpy(start), kind))
             want.append(full)
-        cache = {}
-        partition.exchange_rows(plan, bufs, index_cache=cache)
-        partition.exchange_rows(plan, bufs, index_cache=cache)   # idempotent on owner truth
+        packer = partition.TorchRows(bufs)
+        partition.exchange_packed(plan, packer)
+        partition.exchange_packed(plan, packer)   # idempotent on owner truth
         ok = all(np.array_equal(b.numpy(), w) for (b, _), w in zip(bufs, want))
         open(os.path.join(result_dir, f"rank{rank}"), "w").write("ok" if ok else "bad")
     finally:

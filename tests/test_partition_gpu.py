@@ -132,3 +132,49 @@ def test_exchange_hook_failure_and_refusals(arrays):
                        {k: getattr(gside, k) for k in _lib.SIDECAR_FIELDS}), want) == {}
     drv.capture_graph()   # no hook: the graph is allowed again
     drv.close()
+
+
+def test_halo_pack_and_unpack_move_exactly_the_listed_rows(arrays):
+    """The one-launch halo kernels against torch indexing: cell, edge and
+    tracer buffers, random row lists; unpack writes those rows only."""
+    import torch
+
+    lib = _lib.load()
+    drv = hexdyn.from_case(arrays_case(arrays), _config(False))
+    s = drv.sizes
+    S, nC, nE, T = drv.level_stride, s["n_cells"], s["n_edges"], s["n_scalars"]
+    g = torch.Generator(device="cuda").manual_seed(0)
+    shapes = [(1, nC), (1, nE), (T, nC), (1, nC)]
+    kinds = [_lib.KIND_CELL, _lib.KIND_EDGE, _lib.KIND_TRACER, _lib.KIND_CELL]
+    bufs = [torch.randn(b, n, S, device="cuda", generator=g) for b, n in shapes]
+    crow = torch.randperm(nC, device="cuda", generator=g)[:777].to(torch.int32)
+    erow = torch.randperm(nE, device="cuda", generator=g)[:1234].to(torch.int32)
+    ptrs = (C.c_void_p * 4)(*[b.data_ptr() for b in bufs])
+    kind_arr = (C.c_int * 4)(*kinds)
+    words = lib.hexdyn_halo_words(drv._handle, 4, kind_arr, 777, 1234)
+    assert words == (777 + 1234 + T * 777 + 777) * S
+    packed = torch.empty(words, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(lib.hexdyn_halo_pack(drv._handle, 4, ptrs, kind_arr, C.c_void_p(crow.data_ptr()), 777,
+                                    C.c_void_p(erow.data_ptr()), 1234, C.c_void_p(packed.data_ptr()), st))
+    want = torch.cat([b[:, (erow if k == _lib.KIND_EDGE else crow).long()].reshape(-1) for b, k in zip(bufs, kinds)])
+    assert torch.equal(packed, want)
+    dst = [torch.zeros_like(b) for b in bufs]
+    dptrs = (C.c_void_p * 4)(*[b.data_ptr() for b in dst])
+    _lib.check(lib.hexdyn_halo_unpack(drv._handle, 4, dptrs, kind_arr, C.c_void_p(crow.data_ptr()), 777,
+                                      C.c_void_p(erow.data_ptr()), 1234, C.c_void_p(packed.data_ptr()), st))
+    for b, d, k in zip(bufs, dst, kinds):
+        rows = (erow if k == _lib.KIND_EDGE else crow).long()
+        mask = torch.zeros(b.shape[1], dtype=torch.bool, device="cuda")
+        mask[rows] = True
+        assert torch.equal(d[:, mask], b[:, mask]) and not d[:, ~mask].any()
+    # refusals, before any launch
+    many = (C.c_void_p * 25)(*([bufs[0].data_ptr()] * 25))
+    many_kinds = (C.c_int * 25)(*([_lib.KIND_CELL] * 25))
+    assert lib.hexdyn_halo_pack(drv._handle, 25, many, many_kinds, C.c_void_p(crow.data_ptr()), 777, None, 0,
+                                C.c_void_p(packed.data_ptr()), st) == _lib.HEXDYN_E_ARG
+    odd = (C.c_void_p * 1)(bufs[0].data_ptr() + 4)
+    assert lib.hexdyn_halo_pack(drv._handle, 1, odd, kind_arr, C.c_void_p(crow.data_ptr()), 777, None, 0,
+                                C.c_void_p(packed.data_ptr()), st) == _lib.HEXDYN_E_ARG
+    torch.cuda.synchronize()
+    drv.close()

@@ -1,7 +1,7 @@
 """Oracle (test infrastructure only): the MPAS-A v8.4.1/8.4.2 dry-plus-tracer
 dycore step, restated in vectorised NumPy FP32.
 
-This is the checker the CUDA path is compared against.  Nothing in the
+The CUDA path is compared against it in the tests.  Nothing in the
 product imports it.  It restates the reference's CPU authority
 (``DryDycoreDriver.step`` with ``V841DryDycoreConfig``), operation for
 operation and in the same order, so that its FP32 results are bit-identical:

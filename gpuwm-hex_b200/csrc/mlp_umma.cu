@@ -184,7 +184,8 @@ struct Gemm {
 
 // Epilogue of 8 accumulator columns of one row: bias, then the selected
 // epilogue, stores of C / C^T / Z / Cf (shared by both GEMM kernels).
-__device__ __forceinline__ void epilogue8(const Gemm& p, int row, int col, float* v) {
+__device__ __forceinline__ void epilogue8(const Gemm& p, int row, int col, float* v, uint4* c_out = nullptr,
+                                          float4* f_out = nullptr) {
   if (p.bias) {
     // the same 8 bias words for every lane of the warp: two broadcast 128-bit loads
     const float4 b0 = __ldg(reinterpret_cast<const float4*>(p.bias + col));
@@ -206,7 +207,10 @@ __device__ __forceinline__ void epilogue8(const Gemm& p, int row, int col, float
       h[i] = __float2bfloat16_rn(gelu(v[i]));
     }
     if (p.Z) *reinterpret_cast<uint4*>(p.Z + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(z);
-    if (p.C) *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(h);
+    if (c_out)
+      *c_out = *reinterpret_cast<uint4*>(h);  // the caller stores C
+    else if (p.C)
+      *reinterpret_cast<uint4*>(p.C + (size_t)row * p.N + col) = *reinterpret_cast<uint4*>(h);
     if (p.Ct) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = h[i];
@@ -223,7 +227,7 @@ __device__ __forceinline__ void epilogue8(const Gemm& p, int row, int col, float
       for (int i = 0; i < 8; ++i) p.Ct[(size_t)(col + i) * p.M + row] = d[i];
     }
   } else {
-    float4* dst = reinterpret_cast<float4*>(p.Cf + (size_t)row * p.N + col);
+    float4* dst = f_out ? f_out : reinterpret_cast<float4*>(p.Cf + (size_t)row * p.N + col);  // f_out: caller stores
     dst[0] = make_float4(v[0], v[1], v[2], v[3]);
     dst[1] = make_float4(v[4], v[5], v[6], v[7]);
     if (p.C) {
@@ -365,6 +369,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_gemm_bf16(Gemm p) {
 // asynchronous copy or MMA is in flight at exit on either path.
 constexpr int WS_THREADS = 320;
 constexpr int WS_STAGES = 4;
+constexpr int STAGE_ROW = 80;  // bytes between rows of an epilogue warp's staging tile
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
@@ -498,6 +503,11 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   } else {
     // epilogue warps 2..9: lane quarter warp % 4, column half (warp - 2) / 4
     const int quarter = warp & 3, half = (warp - 2) >> 2;
+    // bf16 activations leave through a per-warp staging tile (32 rows of 64
+    // bytes, rows 80 bytes apart) so that the global stores are row-contiguous
+    const bool staged = p.epilogue == HEXMLP_EPI_GELU && p.C != nullptr;
+    const bool staged_f32 = p.epilogue == HEXMLP_EPI_F32 && p.C == nullptr;
+    uint8_t* stage_tile = smem + WS_STAGES * STAGE + 256 + (warp - 2) * 32 * STAGE_ROW;
     int tc = 0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tc) {
       const int b = tc & 1;
@@ -516,8 +526,47 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       for (int c32 = half * (BN / 2); c32 < (half + 1) * (BN / 2); c32 += 32) {
         float v32[32];
         tmem_ld32(base + (uint32_t)c32, v32);
+        if (staged) {
+          // this lane's row of 32 activations into the warp's staging tile,
+          // then out row by row: 4 lanes write a row's 64 contiguous bytes
 #pragma unroll
-        for (int g8 = 0; g8 < 4; ++g8) epilogue8(p, row, n0 + c32 + 8 * g8, v32 + 8 * g8);
+          for (int g8 = 0; g8 < 4; ++g8) {
+            uint4 h;
+            epilogue8(p, row, n0 + c32 + 8 * g8, v32 + 8 * g8, &h);
+            *reinterpret_cast<uint4*>(stage_tile + lane * STAGE_ROW + 16 * g8) = h;
+          }
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int r = 8 * j + (lane >> 2), piece = lane & 3;
+            const uint4 h = *reinterpret_cast<const uint4*>(stage_tile + r * STAGE_ROW + 16 * piece);
+            *reinterpret_cast<uint4*>(p.C + (size_t)(m0 + quarter * 32 + r) * p.N + n0 + c32 + 8 * piece) = h;
+          }
+          __syncwarp();
+        } else if (staged_f32) {
+          // FP32 out: two halves of 16 columns (64 bytes a row) through the tile
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+#pragma unroll
+            for (int g = 0; g < 2; ++g) {
+              const int g8 = 2 * hh + g;
+              epilogue8(p, row, n0 + c32 + 8 * g8, v32 + 8 * g8, nullptr,
+                        reinterpret_cast<float4*>(stage_tile + lane * STAGE_ROW + 32 * g));
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int r = 8 * j + (lane >> 2), piece = lane & 3;
+              const float4 f = *reinterpret_cast<const float4*>(stage_tile + r * STAGE_ROW + 16 * piece);
+              *reinterpret_cast<float4*>(p.Cf + (size_t)(m0 + quarter * 32 + r) * p.N + n0 + c32 + 16 * hh +
+                                         4 * piece) = f;
+            }
+            __syncwarp();
+          }
+        } else {
+#pragma unroll
+          for (int g8 = 0; g8 < 4; ++g8) epilogue8(p, row, n0 + c32 + 8 * g8, v32 + 8 * g8);
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
@@ -665,7 +714,7 @@ bool make_map(CUtensorMap* m, const void* base, int rows, int K, int box_rows) {
 
 template <int BN>
 size_t ws_smem_bytes() {
-  return (size_t)WS_STAGES * (BM + BN) * BK * 2 + 1024 + 256;
+  return (size_t)WS_STAGES * (BM + BN) * BK * 2 + 1024 + 256 + 8 * 32 * STAGE_ROW;
 }
 
 template <int BN>

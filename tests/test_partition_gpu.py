@@ -178,3 +178,28 @@ def test_halo_pack_and_unpack_move_exactly_the_listed_rows(arrays):
                                 C.c_void_p(packed.data_ptr()), st) == _lib.HEXDYN_E_ARG
     torch.cuda.synchronize()
     drv.close()
+
+
+def test_rank_dycore_runs_over_nccl(arrays):
+    """The one-rank-per-GPU runner through its NCCL process group: here one
+    rank (every GPU call of this suite has one GPU), so it owns the whole
+    mesh, posts no transfers, and steps as the single instance does."""
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", str(29400 + os.getpid() % 500))
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        cfg = _config(False)
+        want = _single(arrays, cfg, 2)
+        rank = partition.RankDycore(arrays, cfg)
+        assert rank.plan.peers() == [] and rank.layout.n_owned["cell"] == arrays["mesh.areaCell"].size
+        for step in range(2):
+            rank.step(1)
+            assert _differing(rank.get_state(), want[step]) == {}, step
+        rank.close()
+    finally:
+        dist.destroy_process_group()

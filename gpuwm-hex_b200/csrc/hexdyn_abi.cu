@@ -813,10 +813,20 @@ int hexdyn_autotune(HexDynHandle* h, void* stream, int steps_per_candidate, char
     c.parity = parity0;
     for (auto& x : saved) cudaMemcpyAsync(x.dev, x.copy, x.bytes, cudaMemcpyDeviceToDevice, st);
   };
-  const int candidates[3] = {64, 128, 256};
-  std::vector<std::pair<std::string, double>> times[3];
+  // block sizes tried per launch label (a level-vector block holds
+  // threads / (S/4) cells or edges, a column-group block threads / G columns)
+#ifndef HEX_TUNE_CANDIDATES
+#if HEX_TUNE_THREE
+#define HEX_TUNE_CANDIDATES 64, 128, 256
+#else
+#define HEX_TUNE_CANDIDATES 64, 96, 128, 160, 192, 224, 256
+#endif
+#endif
+  const int candidates[] = {HEX_TUNE_CANDIDATES};
+  constexpr int NC = (int)(sizeof(candidates) / sizeof(candidates[0]));
+  std::vector<std::pair<std::string, double>> times[NC];
   cudaError_t err = cudaSuccess;
-  for (int ci = 0; ci < 3 && err == cudaSuccess; ++ci) {
+  for (int ci = 0; ci < NC && err == cudaSuccess; ++ci) {
     restore();
     c.force_threads = candidates[ci];
     err = profile_means(h, st, steps_per_candidate, times[ci]);
@@ -828,26 +838,31 @@ int hexdyn_autotune(HexDynHandle* h, void* stream, int steps_per_candidate, char
   cudaMemsetAsync(c.w.flag, 0, sizeof(int), st);
   if (err != cudaSuccess) return cuda_fail(err, "autotune step");
   if (se != cudaSuccess) return cuda_fail(se, "autotune restore");
-  // the fastest block size of every label
-  std::string text;
+  // the fastest block size of every label; the report's first line lists
+  // the candidates, then one line per label: its mean microseconds at each
+  // candidate and the choice
+  std::string text = "threads";
+  for (int ci = 0; ci < NC; ++ci) text += " " + std::to_string(candidates[ci]);
+  text += "\n";
   std::vector<std::pair<std::string, int>> tuned;
-  for (const auto& lab : times[2]) {
+  for (const auto& lab : times[NC - 1]) {
     double best = 1e30;
-    int best_t = 256;
-    double t3[3] = {0.0, 0.0, 0.0};
-    for (int ci = 0; ci < 3; ++ci)
+    int best_t = candidates[NC - 1];
+    std::string line = lab.first;
+    for (int ci = 0; ci < NC; ++ci) {
+      double t = 0.0;
       for (const auto& x : times[ci])
-        if (x.first == lab.first) {
-          t3[ci] = x.second;
-          if (x.second < best) {
-            best = x.second;
-            best_t = candidates[ci];
-          }
-        }
+        if (x.first == lab.first) t = x.second;
+      if (t > 0.0 && t < best) {
+        best = t;
+        best_t = candidates[ci];
+      }
+      char num[32];
+      snprintf(num, sizeof num, " %.3f", 1000.0 * t);
+      line += num;
+    }
+    line += " " + std::to_string(best_t) + "\n";
     tuned.emplace_back(lab.first, best_t);
-    char line[256];
-    snprintf(line, sizeof line, "%s %.3f %.3f %.3f %d\n", lab.first.c_str(), 1000.0 * t3[0], 1000.0 * t3[1],
-             1000.0 * t3[2], best_t);
     text += line;
   }
   c.tuned_threads = tuned;

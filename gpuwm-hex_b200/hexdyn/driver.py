@@ -249,14 +249,17 @@ class HexDycoreDriver:
     def autotune(self, steps_per_candidate: int = 2) -> dict[str, dict]:
         """Choose the block size of every kernel launch by timing (see
         ``hexdyn_autotune``); the state is left as it was.  Returns, per
-        launch label, the microseconds at 64/128/256 threads and the choice."""
+        launch label, the microseconds at each block size tried and the
+        choice."""
         buf = C.create_string_buffer(1 << 16)
         _lib.check(self._lib.hexdyn_autotune(self._handle, self._stream_handle(), int(steps_per_candidate), buf,
                                              len(buf)))
+        lines = buf.value.decode().splitlines()
+        candidates = [int(x) for x in lines[0].split()[1:]]
         out = {}
-        for line in buf.value.decode().splitlines():
-            name, t64, t128, t256, chosen = line.split()
-            out[name] = {"us": {64: float(t64), 128: float(t128), 256: float(t256)}, "threads": int(chosen)}
+        for line in lines[1:]:
+            parts = line.split()
+            out[parts[0]] = {"us": {t: float(x) for t, x in zip(candidates, parts[1:-1])}, "threads": int(parts[-1])}
         return out
 
     def bind_state(self, tensors: dict | None) -> None:

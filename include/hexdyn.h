@@ -206,12 +206,14 @@ int hexdyn_profile_steps(HexDynHandle* h, void* stream, int nsteps, char* out, s
 
 /* Autotuner of launch shapes (no counterpart in the reference, whose
  * kernels launch fixed shapes): times every kernel of `steps_per_candidate`
- * eager steps with 64, 128 and 256 threads per block (CUDA events per
- * launch), keeps the fastest block size of every launch label, and restores
- * the state and sidecar the steps started from; captured graphs are
- * captured again with the tuned shapes.  Results do not depend on the block
- * size (every entity is computed by the same code).  `report` receives one
- * line per label: "label us@64 us@128 us@256 chosen". */
+ * eager steps with 64, 96, 128, 160, 192, 224 and 256 threads per block
+ * (CUDA events per launch; a block holds threads / (S/4) cells or edges, or
+ * threads / 16 columns in the column sweeps), keeps the fastest block size of
+ * every launch label, and restores the state and sidecar the steps started
+ * from; captured graphs are captured again with the tuned shapes.  Results
+ * do not depend on the block size (every entity is computed by the same
+ * code).  `report` receives "threads <candidates>" and then one line per
+ * label: "label <us at each candidate> chosen". */
 int hexdyn_autotune(HexDynHandle* h, void* stream, int steps_per_candidate, char* report, size_t len);
 
 /* Capture the whole large step into CUDA graphs (one per buffer parity);

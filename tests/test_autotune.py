@@ -22,7 +22,8 @@ def test_autotune_keeps_state_and_results():
     tuned = hexdyn.from_case(case_from_arrays(arr), cfg, capture_graph=True)
     before, side_before = tuned.get_state()
     report = tuned.autotune(steps_per_candidate=1)
-    assert report and all(v["threads"] in (64, 128, 256) for v in report.values())
+    sizes = (64, 96, 128, 160, 192, 224, 256)
+    assert report and all(v["threads"] in sizes and tuple(v["us"]) == sizes for v in report.values())
     assert "k_tend_u" in report and "k_ac_cell_first" in report
     after, side_after = tuned.get_state()
     for k in STATE:

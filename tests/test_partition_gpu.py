@@ -203,3 +203,29 @@ def test_rank_dycore_runs_over_nccl(arrays):
         rank.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("label", ["dry", "native"])
+def test_partitioned_steps_are_the_reference_outputs(label):
+    """Two ranks of the 162-cell, 12-level case with qv + 5 condensates
+    (tests/golden fixture made by the reference itself): the assembled owned
+    regions are the reference's own two steps, word for word."""
+    import torch
+
+    from fixtures import SCALAR_VARIANTS, inputs, load_golden
+
+    assert torch.cuda.is_available()
+    torch.cuda.set_device(0)
+    name, steps = SCALAR_VARIANTS[0]
+    fx = load_golden(name)
+    arr = inputs(fx)
+    cfg = DycoreConfig(config_dt=float(fx["config.dt"]), config_number_of_sub_steps=int(fx["config.n_sub_steps"]),
+                       moist_coefficients=label)
+    part = partition.PartitionedDycore(arr, cfg, 2)
+    for step in range(1, steps + 1):
+        part.step(1)
+        st, sd = part.get_state()
+        want = ({k: fx[f"{label}.step{step}.{k}"] for k in _lib.STATE_FIELDS},
+                {k: fx[f"{label}.step{step}.side.{k}"] for k in _lib.SIDECAR_FIELDS})
+        assert _differing((st, sd), want) == {}, (label, step)
+    part.close()

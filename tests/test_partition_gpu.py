@@ -132,6 +132,10 @@ def test_exchange_hook_failure_and_refusals(arrays):
                        {k: getattr(gside, k) for k in _lib.SIDECAR_FIELDS}), want) == {}
     drv.capture_graph()   # no hook: the graph is allowed again
     drv.close()
+    # ensembles take no exchange hook (a partitioned instance is one member)
+    ens = hexdyn.HexEnsemble.from_cases([arrays_case(arrays), arrays_case(arrays)], cfg)
+    assert lib.hexdyn_set_exchange_hook(ens._handle, noop, None) == _lib.HEXDYN_E_ARG
+    ens.close()
 
 
 def test_halo_pack_and_unpack_move_exactly_the_listed_rows(arrays):

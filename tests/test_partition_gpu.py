@@ -233,3 +233,34 @@ def test_partitioned_steps_are_the_reference_outputs(label):
                 {k: fx[f"{label}.step{step}.side.{k}"] for k in _lib.SIDECAR_FIELDS})
         assert _differing((st, sd), want) == {}, (label, step)
     part.close()
+
+
+def test_a_failing_rank_stops_every_rank_and_publishes_nothing(arrays):
+    """A rank whose exchange fails (an exception on the host, at the first
+    acoustic exchange) breaks the ranks' barrier: every rank's step returns
+    with an error, no state changes, and the instance steps normally after."""
+    cfg = _config(False)
+    part = partition.PartitionedDycore(arrays, cfg, 2, barrier_timeout=60.0)
+    before = part.get_state()
+    good = part._hooks[1]
+    calls = []
+
+    def failing(user, point, nbufs, bufs, kinds):
+        calls.append(point)
+        if point == _lib.XCH_ACOUSTIC:
+            part._errors.append(RuntimeError("rank 1 lost its peer"))
+            part._barrier.abort()
+            return -1
+        return good(user, point, nbufs, bufs, kinds)
+
+    part._hooks[1] = _lib.EXCHANGE_HOOK(failing)
+    with pytest.raises(RuntimeError, match="lost its peer"):
+        part.step(1)
+    assert _lib.XCH_ACOUSTIC in calls
+    after = part.get_state()
+    assert _differing(after, before) == {}
+    part._hooks[1] = good
+    want = _single(arrays, cfg, 1)
+    part.step(1)
+    assert _differing(part.get_state(), want[0]) == {}
+    part.close()
